@@ -1,0 +1,417 @@
+// The two executors, templated on a loop adapter (loops.cuh).
+//
+// (a) Global atomics (FOT_EXEC_ATOMIC) -- replaces the reference's
+//     global-colouring executor (problem.hpp:90-194, one launch and one
+//     cudaDeviceSynchronize per colour).  One launch per iteration, one thread
+//     per cell, mapping rows read as vectors, read sets gathered straight from
+//     HBM/L2, increments added with native atomics (f64 RED; one 16-byte f32x4
+//     RED per row for the FP32 loop).  With warp aggregation, lanes whose
+//     slot targets the same point are grouped with __match_any_sync and summed
+//     in registers by a segmented shuffle tree before one lane issues the
+//     atomics.
+//
+// (b) Hierarchical colouring (FOT_EXEC_HIER / _HIER_LAUNCH) -- replaces
+//     loopGPUHierarchical (problem.hpp:198-339) and its kernels
+//     (e.g. res_calc.hpp:218-383).  A block of cells is one CTA tile.  The
+//     CTA stages the read rows of the block's unique points into shared memory
+//     with cp.async, computes every cell's increments, adds them into a
+//     zeroed shared accumulator in thread-colour order (one __syncthreads per
+//     thread colour) and finally adds the accumulator to point dataset 0 in
+//     HBM.  Blocks of one block colour write disjoint points.  In the
+//     persistent form (FOT_EXEC_HIER) CTAs claim tiles from a queue stored in
+//     block-colour order (and iteration after iteration); a tile computes
+//     immediately -- the loops never read the dataset they increment -- and
+//     only its write-back waits, with a bounded spin, until every tile of the
+//     earlier colours has written back.  The result is therefore
+//     deterministic and equal to replaying the colours in order on the CPU.
+#pragma once
+
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace fot {
+
+// Device view of a problem's data for one run (current cell order).
+struct LoopData {
+  const uint32_t *map[2]; // class 0 = mapping 0; class 1 = a second distinct mapping
+  const void *point[4];   // point datasets by set index
+  void *out;              // point dataset 0
+  void *cell[8];          // cell datasets (SOA, stride n_cells)
+  uint32_t n_points[4];
+  uint32_t n_cells;
+};
+
+// Device view of a hierarchical plan.
+struct HierPlanDev {
+  const uint32_t *block_start; // n_blocks+1 positions
+  const uint32_t *block_wait;  // tiles of earlier colours (per block)
+  const uint8_t *block_ntcol;  // thread colours per block
+  const uint8_t *tcol;         // thread colour per position
+  const uint32_t *pts_off[2];  // per class: n_blocks+1 offsets
+  const uint32_t *pts[2];      // per class: unique points of each block
+  const uint16_t *lidx[2];     // per class: kDim x n_cells local indices (SOA)
+  uint32_t n_blocks;
+  uint32_t total_tiles;        // iterations * n_blocks (persistent form)
+  uint32_t read_off[4];        // shared-memory byte offset of each read set
+  uint32_t acc_off;            // shared-memory byte offset of the accumulator
+  Ctl *ctl;
+};
+
+// Direct (cell) data of one cell: SOA with stride n_cells.
+struct Direct {
+  void *const *base;
+  uint32_t idx;
+  unsigned stride;
+  template <class T> __device__ __forceinline__ const T *ptr(int j) const {
+    return static_cast<const T *>(base[j]) + idx;
+  }
+  template <class T> __device__ __forceinline__ T *wptr(int j) const {
+    return static_cast<T *>(base[j]) + idx;
+  }
+};
+
+// Read rows straight from global memory (problem layout AOS or SOA).
+template <class L, bool SOA> struct GlobalRows {
+  using T = typename L::read_t;
+  const T *base[L::kNumRead > 0 ? L::kNumRead : 1];
+  unsigned np[L::kNumRead > 0 ? L::kNumRead : 1];
+  uint32_t p[2][L::kDim];
+  template <int R> __device__ __forceinline__ const T *ptr(int s) const {
+    const uint32_t q = p[L::read_class(R)][s];
+    return base[R] + (SOA ? (size_t)q : (size_t)q * L::read_dim(R));
+  }
+  template <int R> __device__ __forceinline__ unsigned stride() const {
+    return SOA ? np[R] : 1u;
+  }
+};
+
+// Read rows staged in shared memory (AOS rows, stride 1).
+template <class L> struct SmemRows {
+  using T = typename L::read_t;
+  const T *base[L::kNumRead > 0 ? L::kNumRead : 1];
+  uint16_t l[2][L::kDim];
+  template <int R> __device__ __forceinline__ const T *ptr(int s) const {
+    return base[R] + (uint32_t)l[L::read_class(R)][s] * L::read_dim(R);
+  }
+  template <int R> __device__ __forceinline__ unsigned stride() const { return 1u; }
+};
+
+template <class L, int I = 0, class F>
+__device__ __forceinline__ void static_for_read(F &&f) {
+  if constexpr (I < L::kNumRead) {
+    f(std::integral_constant<int, I>{});
+    static_for_read<L, I + 1>(f);
+  }
+}
+
+__device__ __forceinline__ size_t out_index(bool soa, uint32_t np0, uint32_t p,
+                                            int dim, int k) {
+  return soa ? (size_t)k * np0 + p : (size_t)p * dim + k;
+}
+
+// Load mapping row `c` of a class into q[kDim] with vector loads.
+template <int D>
+__device__ __forceinline__ void load_row(const uint32_t *__restrict__ map, uint32_t c,
+                                         uint32_t (&q)[D]) {
+  if constexpr (D == 2) {
+    const uint2 v = __ldg(reinterpret_cast<const uint2 *>(map) + c);
+    q[0] = v.x;
+    q[1] = v.y;
+  } else if constexpr (D == 4) {
+    const uint4 v = __ldg(reinterpret_cast<const uint4 *>(map) + c);
+    q[0] = v.x; q[1] = v.y; q[2] = v.z; q[3] = v.w;
+  } else if constexpr (D == 8) {
+    const uint4 a = __ldg(reinterpret_cast<const uint4 *>(map) + 2 * (size_t)c);
+    const uint4 b = __ldg(reinterpret_cast<const uint4 *>(map) + 2 * (size_t)c + 1);
+    q[0] = a.x; q[1] = a.y; q[2] = a.z; q[3] = a.w;
+    q[4] = b.x; q[5] = b.y; q[6] = b.z; q[7] = b.w;
+  } else {
+#pragma unroll
+    for (int s = 0; s < D; ++s) q[s] = __ldg(map + (size_t)c * D + s);
+  }
+}
+
+// ===========================================================================
+// (a) atomic executor
+// ===========================================================================
+
+template <class T> __device__ __forceinline__ void atomic_add(T *a, T v) { atomicAdd(a, v); }
+
+template <class L, bool SOA, bool AGG>
+__global__ void __launch_bounds__(256) k_atomic(LoopData d) {
+  using out_t = typename L::out_t;
+  constexpr int D = L::kDim, K = L::kOut;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+  out_t *__restrict__ out = static_cast<out_t *>(d.out);
+  for (uint32_t base = warp * 32u; base < d.n_cells; base += n_warps * 32u) {
+    const uint32_t c = base + lane;
+    const bool valid = c < d.n_cells;
+    GlobalRows<L, SOA> rows;
+    out_t inc[D][K];
+#pragma unroll
+    for (int s = 0; s < D; ++s) {
+      rows.p[0][s] = 0;
+      rows.p[1][s] = 0;
+#pragma unroll
+      for (int k = 0; k < K; ++k) inc[s][k] = out_t(0);
+    }
+    if (valid) {
+      load_row<D>(d.map[0], c, rows.p[0]);
+      if constexpr (L::kHasClass1) load_row<D>(d.map[1], c, rows.p[1]);
+      static_for_read<L>([&](auto r) {
+        constexpr int R = decltype(r)::value;
+        rows.base[R] = static_cast<const typename L::read_t *>(d.point[L::read_set(R)]);
+        rows.np[R] = d.n_points[L::read_set(R)];
+      });
+      Direct dir{d.cell, c, d.n_cells};
+      L::cell(rows, dir, inc);
+    }
+#pragma unroll
+    for (int s = 0; s < D; ++s) {
+      const uint32_t key = valid ? rows.p[0][s] : 0xFFFFFFFFu;
+      bool leader = valid;
+      if constexpr (AGG) {
+        const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
+        const unsigned lt = (1u << lane) - 1u;
+        const int rank = __popc(peers & lt);
+        const int cnt = __popc(peers);
+        const int maxcnt = (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)cnt);
+        for (int off = 1; off < maxcnt; off <<= 1) {
+          const bool has = rank + off < cnt;
+          const int src = has ? (int)__fns(peers, 0, rank + off + 1) : (int)lane;
+          const bool take = has && (rank % (2 * off)) == 0;
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            const out_t v = __shfl_sync(0xFFFFFFFFu, inc[s][k], src);
+            if (take) inc[s][k] += v;
+          }
+        }
+        leader = valid && rank == 0;
+      }
+      if (leader) {
+        if constexpr (!SOA && sizeof(out_t) == 4 && K == 4) {
+          float4 v = make_float4(inc[s][0], inc[s][1], inc[s][2], inc[s][3]);
+          atomicAdd(reinterpret_cast<float4 *>(out) + key, v);
+        } else {
+#pragma unroll
+          for (int k = 0; k < K; ++k)
+            atomic_add(out + out_index(SOA, d.n_points[0], key, K, k), inc[s][k]);
+        }
+      }
+    }
+  }
+}
+
+// ===========================================================================
+// (b) hierarchical executor
+// ===========================================================================
+
+// One tile: block b of plan P.  With WAIT, the write-back first waits until
+// *done >= wait_target (bounded; on timeout *err gets kErrWaitLimit and the
+// tile skips its write-back).
+template <class L, bool SOA, int THREADS, bool WAIT>
+__device__ __forceinline__ void hier_tile(const LoopData &d, const HierPlanDev &P,
+                                          unsigned char *smem, uint32_t b,
+                                          uint32_t wait_target, unsigned int *done,
+                                          unsigned int *err, int &abort) {
+  using out_t = typename L::out_t;
+  using read_t = typename L::read_t;
+  constexpr int D = L::kDim, K = L::kOut;
+  const uint32_t tid = threadIdx.x;
+  const uint32_t start = P.block_start[b];
+  const uint32_t ncell = P.block_start[b + 1] - start;
+  const uint32_t off0 = P.pts_off[0][b];
+  const uint32_t n0 = P.pts_off[0][b + 1] - off0;
+  const uint32_t *__restrict__ pts0 = P.pts[0] + off0;
+  uint32_t off1 = 0, n1 = 0;
+  const uint32_t *__restrict__ pts1 = nullptr;
+  if constexpr (L::kHasClass1) {
+    off1 = P.pts_off[1][b];
+    n1 = P.pts_off[1][b + 1] - off1;
+    pts1 = P.pts[1] + off1;
+  }
+  const uint32_t ntcol = P.block_ntcol[b];
+
+  // 1. stage the read rows of the block's unique points (cp.async)
+  static_for_read<L>([&](auto r) {
+    constexpr int R = decltype(r)::value;
+    constexpr int DIM = L::read_dim(R);
+    constexpr int ROW = DIM * (int)sizeof(read_t);
+    const uint32_t n = L::read_class(R) == 0 ? n0 : n1;
+    const uint32_t *__restrict__ pts = L::read_class(R) == 0 ? pts0 : pts1;
+    const char *src = static_cast<const char *>(d.point[L::read_set(R)]);
+    char *dst = reinterpret_cast<char *>(smem + P.read_off[R]);
+    if constexpr (!SOA) {
+      if constexpr (ROW % 16 == 0) {
+        constexpr int CH = ROW / 16;
+        for (uint32_t e = tid; e < n * CH; e += THREADS) {
+          const uint32_t i = e / CH, c = e - i * CH;
+          cp_async16(dst + (size_t)i * ROW + c * 16, src + (size_t)pts[i] * ROW + c * 16);
+        }
+      } else if constexpr (ROW % 8 == 0) {
+        constexpr int CH = ROW / 8;
+        for (uint32_t e = tid; e < n * CH; e += THREADS) {
+          const uint32_t i = e / CH, c = e - i * CH;
+          cp_async8(dst + (size_t)i * ROW + c * 8, src + (size_t)pts[i] * ROW + c * 8);
+        }
+      } else {
+        constexpr int CH = ROW / 4;
+        for (uint32_t e = tid; e < n * CH; e += THREADS) {
+          const uint32_t i = e / CH, c = e - i * CH;
+          cp_async4(dst + (size_t)i * ROW + c * 4, src + (size_t)pts[i] * ROW + c * 4);
+        }
+      }
+    } else {
+      const uint32_t np = d.n_points[L::read_set(R)];
+      for (uint32_t e = tid; e < n * DIM; e += THREADS) {
+        const uint32_t k = e / n, i = e - k * n;
+        const char *g = src + ((size_t)k * np + pts[i]) * sizeof(read_t);
+        char *s = dst + ((size_t)i * DIM + k) * sizeof(read_t);
+        if constexpr (sizeof(read_t) == 8) cp_async8(s, g);
+        else cp_async4(s, g);
+      }
+    }
+  });
+  // 2. zero the accumulator while the copies fly
+  out_t *acc = reinterpret_cast<out_t *>(smem + P.acc_off);
+  for (uint32_t e = tid; e < n0 * K; e += THREADS) acc[e] = out_t(0);
+  // 3. per-cell local indices and thread colour (coalesced loads)
+  const bool active = tid < ncell;
+  const uint32_t pos = start + tid;
+  SmemRows<L> rows;
+  uint32_t my_col = 0xFFFFFFFFu;
+  if (active) {
+#pragma unroll
+    for (int s = 0; s < D; ++s) {
+      rows.l[0][s] = P.lidx[0][(size_t)s * d.n_cells + pos];
+      rows.l[1][s] = L::kHasClass1 ? P.lidx[1][(size_t)s * d.n_cells + pos] : 0;
+    }
+    my_col = P.tcol[pos];
+  }
+  static_for_read<L>([&](auto r) {
+    constexpr int R = decltype(r)::value;
+    rows.base[R] = reinterpret_cast<const read_t *>(smem + P.read_off[R]);
+  });
+  cp_async_wait_all();
+  __syncthreads();
+  // 4. compute
+  out_t inc[D][K];
+  if (active) {
+    Direct dir{d.cell, pos, d.n_cells};
+    L::cell(rows, dir, inc);
+  }
+  // 5. accumulate in thread-colour order
+  for (uint32_t col = 0; col < ntcol; ++col) {
+    if (my_col == col) {
+#pragma unroll
+      for (int s = 0; s < D; ++s)
+#pragma unroll
+        for (int k = 0; k < K; ++k) acc[(uint32_t)rows.l[0][s] * K + k] += inc[s][k];
+    }
+    __syncthreads();
+  }
+  // 6. wait until every tile of the earlier colours has written back
+  if constexpr (WAIT) {
+    __shared__ int s_abort;
+    if (tid == 0) {
+      unsigned int polls = 0;
+      int ab = 0;
+      while (ld_acquire_gpu(done) < wait_target) {
+        if (++polls > kWaitPollLimit) {
+          atomicOr(err, kErrWaitLimit);
+          ab = 1;
+          break;
+        }
+        __nanosleep(256);
+      }
+      s_abort = ab;
+    }
+    __syncthreads();
+    abort = s_abort;
+  }
+  // 7. write back: out[p] += acc (L2 loads/stores; L1 may hold stale lines)
+  if (!abort) {
+    out_t *__restrict__ out = static_cast<out_t *>(d.out);
+    if constexpr (!SOA && (K * sizeof(out_t)) % 16 == 0) {
+      constexpr int CH = K * sizeof(out_t) / 16;
+      using vec_t = typename std::conditional<sizeof(out_t) == 8, double2, float4>::type;
+      vec_t *o = reinterpret_cast<vec_t *>(out);
+      const vec_t *a = reinterpret_cast<const vec_t *>(acc);
+      for (uint32_t e = tid; e < n0 * CH; e += THREADS) {
+        const uint32_t i = e / CH, c = e - i * CH;
+        const size_t gi = (size_t)pts0[i] * CH + c;
+        vec_t v = __ldcg(o + gi);
+        const vec_t w = a[e];
+        if constexpr (sizeof(out_t) == 8) {
+          v.x += w.x;
+          v.y += w.y;
+        } else {
+          v.x += w.x;
+          v.y += w.y;
+          v.z += w.z;
+          v.w += w.w;
+        }
+        __stcg(o + gi, v);
+      }
+    } else {
+      for (uint32_t e = tid; e < n0 * K; e += THREADS) {
+        const uint32_t i = e / K, k = e - i * K;
+        const size_t gi = out_index(SOA, d.n_points[0], pts0[i], K, k);
+        __stcg(out + gi, __ldcg(out + gi) + acc[e]);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Persistent form: CTAs claim tiles in colour order until the queue is empty.
+template <class L, bool SOA, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_hier(LoopData d, HierPlanDev P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ uint32_t s_ticket;
+  const uint32_t tid = threadIdx.x;
+  for (;;) {
+    if (tid == 0) {
+      uint32_t t = atomicAdd(&P.ctl->ticket, 1u);
+      if (*(volatile unsigned int *)&P.ctl->error) t = P.total_tiles;
+      s_ticket = t;
+    }
+    __syncthreads();
+    const uint32_t t = s_ticket;
+    if (t >= P.total_tiles) break;
+    const uint32_t iter = t / P.n_blocks;
+    const uint32_t b = t - iter * P.n_blocks;
+    int abort = 0;
+    hier_tile<L, SOA, THREADS, true>(d, P, smem, b, iter * P.n_blocks + P.block_wait[b],
+                                     &P.ctl->done, &P.ctl->error, abort);
+    if (tid == 0) {
+      __threadfence();
+      atomicAdd(&P.ctl->done, 1u);
+    }
+  }
+  // the last CTA to leave resets the queue for the next launch
+  if (tid == 0) {
+    __threadfence();
+    const unsigned int prev = atomicAdd(&P.ctl->exited, 1u);
+    if (prev == gridDim.x - 1) {
+      atomicExch(&P.ctl->ticket, 0u);
+      atomicExch(&P.ctl->done, 0u);
+      atomicExch(&P.ctl->exited, 0u);
+      __threadfence();
+    }
+  }
+}
+
+// One launch per block colour: CTA x handles block first + x, no waiting.
+template <class L, bool SOA, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_hier_colour(LoopData d, HierPlanDev P,
+                                                         uint32_t first) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  int abort = 0;
+  hier_tile<L, SOA, THREADS, false>(d, P, smem, first + blockIdx.x, 0, nullptr, nullptr, abort);
+}
+
+} // namespace fot

@@ -1,0 +1,106 @@
+// Instantiates both executors for the loop selected by FOT_ADAPTER and
+// exposes them through a LoopOps table.  Included once by each loop_*.cu.
+#pragma once
+
+#include "engine.hpp"
+#include "loops.cuh"
+
+namespace fot {
+namespace FOT_ADAPTER_NS {
+
+using L = Loop;
+
+template <bool SOA, bool AGG> int launch_atomic(const LoopData &d, uint32_t threads,
+                                               uint32_t grid, cudaStream_t st) {
+  if (threads != 256) return fail(FOT_ERR_ARG, "atomic executor runs 256 threads per CTA");
+  k_atomic<L, SOA, AGG><<<grid, 256, 0, st>>>(d);
+  FOT_CUDA(cudaGetLastError());
+  return FOT_OK;
+}
+
+int run_atomic(const LoopData &d, bool soa, bool agg, uint32_t threads, uint32_t grid,
+               cudaStream_t st) {
+  if (soa) return agg ? launch_atomic<true, true>(d, threads, grid, st)
+                      : launch_atomic<true, false>(d, threads, grid, st);
+  return agg ? launch_atomic<false, true>(d, threads, grid, st)
+             : launch_atomic<false, false>(d, threads, grid, st);
+}
+
+template <bool SOA, int T> const void *hier_kernel(bool persistent) {
+  return persistent ? reinterpret_cast<const void *>(&k_hier<L, SOA, T>)
+                    : reinterpret_cast<const void *>(&k_hier_colour<L, SOA, T>);
+}
+
+template <bool SOA> const void *hier_kernel_t(bool persistent, uint32_t threads) {
+  switch (threads) {
+  case 128: return hier_kernel<SOA, 128>(persistent);
+  case 256: return hier_kernel<SOA, 256>(persistent);
+  case 512: return hier_kernel<SOA, 512>(persistent);
+  case 1024: return hier_kernel<SOA, 1024>(persistent);
+  }
+  return nullptr;
+}
+
+const void *kernel_for(int exec, bool soa, uint32_t threads) {
+  if (exec == FOT_EXEC_ATOMIC)
+    return soa ? reinterpret_cast<const void *>(&k_atomic<L, true, true>)
+               : reinterpret_cast<const void *>(&k_atomic<L, false, true>);
+  const bool persistent = exec == FOT_EXEC_HIER;
+  return soa ? hier_kernel_t<true>(persistent, threads) : hier_kernel_t<false>(persistent, threads);
+}
+
+int prepare(const void *k, size_t smem) {
+  FOT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  return FOT_OK;
+}
+
+int run_hier(const LoopData &d, const HierPlanDev &P, bool soa, uint32_t threads,
+             uint32_t grid, size_t smem, cudaStream_t st) {
+  const void *k = kernel_for(FOT_EXEC_HIER, soa, threads);
+  if (!k) return fail(FOT_ERR_ARG, "no hierarchical kernel for %u threads", threads);
+  FOT_TRY(prepare(k, smem));
+  void *args[] = {const_cast<LoopData *>(&d), const_cast<HierPlanDev *>(&P)};
+  FOT_CUDA(cudaLaunchKernel(k, dim3(grid), dim3(threads), args, smem, st));
+  return FOT_OK;
+}
+
+int run_hier_colour(const LoopData &d, const HierPlanDev &P, bool soa, uint32_t threads,
+                    uint32_t first, uint32_t count, size_t smem, cudaStream_t st) {
+  const void *k = kernel_for(FOT_EXEC_HIER_LAUNCH, soa, threads);
+  if (!k) return fail(FOT_ERR_ARG, "no hierarchical kernel for %u threads", threads);
+  FOT_TRY(prepare(k, smem));
+  void *args[] = {const_cast<LoopData *>(&d), const_cast<HierPlanDev *>(&P), &first};
+  FOT_CUDA(cudaLaunchKernel(k, dim3(count), dim3(threads), args, smem, st));
+  return FOT_OK;
+}
+
+int occupancy(int exec, bool soa, uint32_t threads, size_t smem, int *per_sm) {
+  const void *k = kernel_for(exec, soa, exec == FOT_EXEC_ATOMIC ? 256 : threads);
+  if (!k) return fail(FOT_ERR_ARG, "no kernel for %u threads", threads);
+  if (exec != FOT_EXEC_ATOMIC) FOT_TRY(prepare(k, smem));
+  FOT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      per_sm, k, exec == FOT_EXEC_ATOMIC ? 256 : (int)threads, smem));
+  return FOT_OK;
+}
+
+size_t smem_layout(uint32_t cap0, uint32_t cap1, uint32_t read_off[4], uint32_t *acc_off) {
+  size_t off = 0;
+  for (int r = 0; r < 4; ++r) read_off[r] = 0;
+  for (int r = 0; r < L::kNumRead; ++r) {
+    read_off[r] = (uint32_t)off;
+    const uint32_t cap = L::read_class(r) == 0 ? cap0 : cap1;
+    off += (size_t)cap * L::read_dim(r) * sizeof(typename L::read_t);
+    off = (off + 15) & ~size_t(15);
+  }
+  *acc_off = (uint32_t)off;
+  off += (size_t)cap0 * L::kOut * sizeof(typename L::out_t);
+  return (off + 15) & ~size_t(15);
+}
+
+} // namespace FOT_ADAPTER_NS
+
+extern const LoopOps FOT_OPS_NAME;
+const LoopOps FOT_OPS_NAME = {FOT_ADAPTER_NS::run_atomic, FOT_ADAPTER_NS::run_hier,
+                              FOT_ADAPTER_NS::run_hier_colour, FOT_ADAPTER_NS::occupancy,
+                              FOT_ADAPTER_NS::smem_layout};
+} // namespace fot

@@ -1,0 +1,245 @@
+/*
+ * fot.h -- C ABI of the B200 indirect-increment loop engine (libfot.so).
+ *
+ * The engine runs the reference's indirect-increment loops (an iteration set
+ * of "cells" -- edges, faces or elements -- each computing an increment from
+ * direct and indirectly-addressed data and adding it to the "points" it maps
+ * to) on one GPU.  It is the drop-in for the reference's Problem / Mesh /
+ * data_t host API (problem.hpp, mesh.hpp, data_t.hpp) and its loop drivers;
+ * include/fot_problem.hpp rebuilds that C++ surface on top of this ABI.
+ *
+ * Conventions
+ *   - Every entry point returns an int status: FOT_OK (0) or a negative
+ *     FOT_ERR_* code; fot_last_error() gives the message of the last failure
+ *     on the calling thread.  Nothing here calls exit() (the reference's
+ *     checkCudaErrors does, helper_cuda.h).
+ *   - Handles are opaque.  A problem and its plans are thread-compatible, not
+ *     thread-safe: use one handle from one thread (or serialise).
+ *   - Streams are passed as void* (a cudaStream_t; NULL = the legacy default
+ *     stream).  Launching calls are asynchronous; fot_sync() waits and reports
+ *     device-side errors.
+ *   - Arrays are plain host pointers with explicit element counts.
+ *   - Types: mappings are uint32 (the reference's MY_SIZE); point and cell
+ *     datasets have the element types of the loop (double, float, int).
+ *
+ * Data layout (the reference's, data_t.hpp:104-114 and kernels/*.hpp):
+ *   mapping k        n_cells x mesh_dim[k] uint32, AOS (cell-major)
+ *   point dataset k  n_points[k] x dim: AOS (point-major) when the problem's
+ *                    layout is FOT_AOS, SOA (component-major) for FOT_SOA
+ *   cell dataset j   always SOA: dim x n_cells
+ * Point dataset 0 is the incremented dataset (point_weights[0]).
+ */
+#ifndef FOT_H
+#define FOT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define FOT_OK 0
+#define FOT_ERR_ARG -1        /* invalid argument / size mismatch */
+#define FOT_ERR_CUDA -2       /* a CUDA runtime call failed */
+#define FOT_ERR_STATE -3      /* stale plan, wrong problem, ... */
+#define FOT_ERR_LIMIT -4      /* an engine limit was exceeded (colours, sizes) */
+#define FOT_ERR_DEVICE -5     /* a kernel reported an error (wait limit hit) */
+#define FOT_ERR_NOMEM -6      /* device allocation failed */
+
+/* loops: the reference's five applications (kernels/*_func.hpp) */
+#define FOT_LOOP_RES_CALC 0  /* Airfoil edge flux, FP64 (kernels/res_calc.hpp) */
+#define FOT_LOOP_MINI_AERO 1 /* miniAero face flux, FP64 (kernels/mini_aero.hpp) */
+#define FOT_LOOP_LULESH 2    /* LULESH hex stress -> node force, FP64 (kernels/lulesh.hpp) */
+#define FOT_LOOP_VOLNA 3     /* Volna edge flux, FP32 (kernels/volna.hpp) */
+#define FOT_LOOP_GETACC 4    /* BookLeaf getacc scatter, FP64 (kernels/getacc_scatter.hpp) */
+#define FOT_NUM_LOOPS 5
+
+/* point-data layout: the reference's Problem<SOA> template parameter */
+#define FOT_AOS 0
+#define FOT_SOA 1
+
+/* executors */
+#define FOT_EXEC_ATOMIC 0      /* one launch, native atomics (+ warp aggregation) */
+#define FOT_EXEC_HIER 1        /* two-level colouring, one persistent launch */
+#define FOT_EXEC_HIER_LAUNCH 2 /* two-level colouring, one launch per block colour */
+
+/* orderings (fot_reorder) */
+#define FOT_ORDER_NATURAL 0 /* keep the point numbering, sort cells by point tuple */
+#define FOT_ORDER_RANDOM 1  /* seeded random point numbering */
+#define FOT_ORDER_RCM 2     /* reverse Cuthill-McKee */
+#define FOT_ORDER_GPS 3     /* Gibbs-Poole-Stockmeyer (in place of SCOTCH "g") */
+
+/* plan flags */
+#define FOT_PLAN_NO_AGGREGATE 1u /* atomic executor: no warp aggregation */
+#define FOT_PLAN_USE_PARTITION 2u /* hierarchical: blocks from the partition */
+
+typedef struct fot_problem fot_problem;
+typedef struct fot_plan fot_plan;
+typedef struct fot_graph fot_graph;
+typedef struct fot_batch fot_batch;
+
+/* Shape of a loop's data: the bindings of the reference drivers' initProblem
+ * (res_calc.cu:10-28, mini_aero.cu:10-24, lulesh.cu:10-24, volna.cu:11-27,
+ * getacc.cu:11-26). */
+typedef struct fot_loop_info {
+  uint32_t n_mappings;
+  uint32_t mesh_dim[4];
+  uint32_t n_point_sets; /* == n_mappings: point dataset k lives on mapping k */
+  uint32_t point_dim[4];
+  uint32_t point_type_size[4];
+  uint32_t n_cell_sets;
+  uint32_t cell_dim[8];
+  uint32_t cell_type_size[8];
+  uint32_t cell_written_mask; /* bit j set: cell dataset j is written (lulesh determ) */
+} fot_loop_info;
+
+/* Describe a loop's bindings.  Replaces the per-driver initProblem. */
+int fot_loop_describe(int loop, fot_loop_info *info);
+
+const char *fot_last_error(void);
+const char *fot_version(void);
+
+/* ---- problem (Problem<SOA> + Mesh + data_t) ---------------------------- */
+
+/* Create a problem on the current CUDA device from host mappings.
+ * Replaces Problem<SOA>(mesh streams, mesh_dim, point_data_params,
+ * cell_data_params, block_size) (problem.hpp:59-77) and the Mesh stream
+ * constructor (mesh.hpp:67-98).  n_points has n_mappings entries, maps[k]
+ * n_cells*mesh_dim[k] entries.  Mappings whose point set the loop reads
+ * through mapping 0 (res_calc 2, 3; mini_aero, lulesh, volna 1) must equal
+ * mapping 0, as in the reference's inputs; the engine then keeps them as one. */
+int fot_problem_create(int loop, int layout, uint32_t n_cells,
+                       const uint32_t *n_points, const uint32_t *const *maps,
+                       fot_problem **out);
+int fot_problem_destroy(fot_problem *p);
+
+/* Upload / download datasets in the problem's CURRENT numbering.
+ * Replace Problem::readPointData / readCellData (problem.hpp:583-632) and
+ * data_t::flushToDevice / flushToHost (data_t.cu:38-56).  bytes must equal
+ * the dataset size.  The stream variants are asynchronous on `stream`
+ * (host memory should be pinned); the plain ones synchronise. */
+int fot_set_point_data(fot_problem *p, uint32_t k, const void *host, size_t bytes);
+int fot_get_point_data(fot_problem *p, uint32_t k, void *host, size_t bytes);
+int fot_set_cell_data(fot_problem *p, uint32_t j, const void *host, size_t bytes);
+int fot_get_cell_data(fot_problem *p, uint32_t j, void *host, size_t bytes);
+int fot_set_point_data_async(fot_problem *p, uint32_t k, const void *host, size_t bytes, void *stream);
+int fot_get_point_data_async(fot_problem *p, uint32_t k, void *host, size_t bytes, void *stream);
+int fot_set_cell_data_async(fot_problem *p, uint32_t j, const void *host, size_t bytes, void *stream);
+
+/* Device address of a dataset (owned by the problem; valid until the problem
+ * is destroyed).  data_t::getDeviceData (data_t.hpp:48-52). */
+int fot_point_data_device(fot_problem *p, uint32_t k, void **dptr);
+int fot_cell_data_device(fot_problem *p, uint32_t j, void **dptr);
+
+/* Current mapping k (n_cells*mesh_dim[k]) and sizes. */
+int fot_get_mapping(fot_problem *p, uint32_t k, uint32_t *host);
+int fot_problem_sizes(const fot_problem *p, uint32_t *n_cells, uint32_t *n_points /* [n_mappings] */);
+
+/* Permutations applied so far.  point_perm[k][orig] = current number of
+ * point `orig` of set k (the reference's applied_permutation, problem.hpp:35,
+ * for k = 0); cell_order[current] = original cell id. */
+int fot_get_point_permutation(fot_problem *p, uint32_t k, uint32_t *host);
+int fot_get_cell_order(fot_problem *p, uint32_t *host);
+
+/* ---- orderings and partitions (GPU plan builders) ----------------------- */
+
+/* Renumber the points of mapping 0 by `order` (seed used by FOT_ORDER_RANDOM),
+ * then sort the cells lexicographically by their sorted point tuples; the
+ * other mappings follow: one equal to mapping 0 takes the same numbering,
+ * another (res_calc's edge->node) is renumbered by first touch in the new cell
+ * order.  Datasets move with their points and cells.  Replaces
+ * Problem::reorder<SameMapping> (problem.hpp:439-482) with Mesh::reorder
+ * (mesh.hpp:199-225) and SCOTCH's GPS ordering (reorder.hpp:135-175). */
+int fot_reorder(fot_problem *p, int order, uint64_t seed);
+
+/* Partition the cells into parts of at most part_size cells by growing
+ * connected parts over the cell-to-cell graph on the GPU.  The partition is
+ * stored on the problem (Problem::partition_vector).  Replaces
+ * Problem::partition / partitionOurs (problem.hpp:484-515) and METIS. */
+int fot_partition(fot_problem *p, uint32_t part_size, uint64_t seed);
+/* Problem::reorderToPartition (problem.hpp:517-526): cells sorted by part. */
+int fot_reorder_to_partition(fot_problem *p);
+/* Problem::renumberPoints (problem.hpp:528-551): points renumbered by the
+ * number of parts touching them (descending) and then by part. */
+int fot_renumber_points(fot_problem *p);
+/* Partition vector (n_cells, current cell order); FOT_ERR_STATE when none. */
+int fot_get_partition(fot_problem *p, uint32_t *host);
+int fot_set_partition(fot_problem *p, const uint32_t *host);
+
+/* ---- plans ---------------------------------------------------------------- */
+
+typedef struct fot_plan_desc {
+  int exec;            /* FOT_EXEC_* */
+  uint32_t block_size; /* cells per block (hierarchical) / threads per CTA (atomic) */
+  uint32_t flags;      /* FOT_PLAN_* */
+  uint32_t reserved;
+} fot_plan_desc;
+
+typedef struct fot_plan_stats {
+  int exec;
+  uint32_t block_size;
+  uint32_t n_blocks;
+  uint32_t n_colours;          /* block colours */
+  uint32_t max_block_points;   /* written points of the largest block */
+  uint32_t max_block_points1;  /* second (read) mapping class, 0 if none */
+  uint32_t max_thread_colours;
+  double avg_thread_colours;
+  double avg_block_points;     /* written points per block */
+  uint64_t plan_bytes;         /* device bytes held by the plan */
+  uint32_t smem_bytes;         /* dynamic shared memory per CTA */
+  uint32_t grid;               /* CTAs per launch */
+  double build_ms;             /* wall time of fot_plan_build */
+} fot_plan_stats;
+
+/* Build an execution plan on the GPU.  For the hierarchical executors this
+ * replaces HierarchicalColourMemory (colouring.hpp:44-147, colouring.cu:12-102)
+ * and REORDERS THE PROBLEM'S CELLS into plan order (blocks by block colour,
+ * cells of a block by thread colour), recorded in fot_get_cell_order, so that
+ * direct data are read coalesced.  A later plan build or reorder makes older
+ * plans stale (fot_run then fails with FOT_ERR_STATE). */
+int fot_plan_build(fot_problem *p, const fot_plan_desc *desc, fot_plan **out);
+int fot_plan_destroy(fot_plan *plan);
+int fot_plan_get_stats(const fot_plan *plan, fot_plan_stats *stats);
+
+/* Export a hierarchical plan into host arrays (for exact checks):
+ * colour_offsets[n_colours+1], block_start[n_blocks+1], cell_id[n_cells]
+ * (original cell of each position), tcol[n_cells], block_ntcol[n_blocks],
+ * pts_off[n_blocks+1], pts[pts_off[n_blocks]], lidx[mesh_dim*n_cells].
+ * Call with pts == NULL to get the sizes only. */
+int fot_plan_export(const fot_plan *plan, uint32_t *n_blocks, uint32_t *n_colours,
+                    uint32_t *n_pts, uint32_t *colour_offsets, uint32_t *block_start,
+                    uint32_t *cell_id, uint8_t *tcol, uint8_t *block_ntcol,
+                    uint32_t *pts_off, uint32_t *pts, uint16_t *lidx);
+
+/* ---- execution ------------------------------------------------------------ */
+
+/* Run `iterations` iterations of the loop, accumulating into point dataset 0
+ * on the device.  Replaces Problem::loopGPUCellCentred (problem.hpp:90-194)
+ * and loopGPUHierarchical (problem.hpp:198-339) without their per-colour
+ * cudaDeviceSynchronize and the per-iteration copy-back.  Asynchronous. */
+int fot_run(fot_problem *p, fot_plan *plan, uint32_t iterations, void *stream);
+/* Wait for the problem's work on `stream` and report device-side errors. */
+int fot_sync(fot_problem *p, void *stream);
+
+/* Capture `iterations` iterations of fot_run into a CUDA graph and replay it. */
+int fot_graph_create(fot_problem *p, fot_plan *plan, uint32_t iterations,
+                     void *stream, fot_graph **out);
+int fot_graph_launch(fot_graph *g, void *stream);
+int fot_graph_destroy(fot_graph *g);
+
+/* ---- batches: many meshes, one persistent launch -------------------------- */
+
+/* Group hierarchical plans of several problems into one persistent launch
+ * over a (mesh, block) tile queue ordered by block colour per mesh. */
+int fot_batch_create(fot_problem *const *problems, fot_plan *const *plans,
+                     uint32_t n, fot_batch **out);
+int fot_batch_run(fot_batch *b, uint32_t iterations, void *stream);
+int fot_batch_sync(fot_batch *b, void *stream);
+int fot_batch_destroy(fot_batch *b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FOT_H */
