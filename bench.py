@@ -1,0 +1,354 @@
+"""Benchmark: indirect-loop GB/s of the tuned plan vs plain atomics.
+
+Workload (one "step" = one iteration of the loop over the whole mesh):
+mini_aero-style 3D face flux, FP64, 128^3 hex cells, 6,242,304 interior faces,
+cell numbering a seeded random permutation; the plan (ordering + executor +
+block size) is picked by the cost model when one is trained and available,
+otherwise by the measured sweep of the autotuner.  GB/s counts the algorithmic
+("unique") bytes of one step: every indirectly read dataset once, the
+incremented dataset read and written once, every direct dataset once, the
+mapping once.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fot|reference]
+
+Multi-GPU: the loop is single-GPU (the engine does not shard a mesh), so N
+GPUs run N independent replicas ("scaling": "weak"); value = the bytes all
+ranks processed / the max over ranks of the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Indirect-loop GB/s (% of HBM roofline), learned-tuned plan vs plain atomics"
+WORKLOAD = "mini_aero 128^3 face flux (FP64), random cell numbering"
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic(kernel_key):
+    """Per-launch DRAM traffic of the dominant kernel from the committed ncu
+    summary (profiles/traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            j = json.load(f)
+        return j.get(kernel_key)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(
+                    ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                     "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.rows.append([v.strip() for v in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for n, v in zip(names, r[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def dist_setup(gpus):
+    import torch
+    if gpus > 1 or "RANK" in os.environ:
+        import torch.distributed as dist
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        return rank, world, local
+    return 0, 1, 0
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_workload(args):
+    from cuda_fot_b200 import meshgen as mg
+    return mg.mini_aero(args.n, seed=args.seed, permute=True)
+
+
+def cpu_baseline(md, impl_kind=None):
+    """The reference's own compiled serial loop (oracle/_ref) on one core, or
+    the oracle port, over a bounded sample: one iteration of the whole mesh."""
+    from oracle import oracle_py as O
+    ub = md.unique_bytes()
+    if O.ref_available():
+        _, _, secs = O.ref_serial(md, 1)
+        kind = "reference"
+    else:
+        t0 = time.perf_counter()
+        O.serial(md, 1)
+        secs = time.perf_counter() - t0
+        kind = "port"
+    return {"value": ub / secs / 1e9, "unit": "GB/s", "cores": 1, "kind": kind,
+            "sample": "1 iteration of the full mesh, serial loop in cell order"}
+
+
+def run_reference(args):
+    """Reference arm: the reference's own CPU loop (OpenMP over its global
+    colouring, all host threads) on the same workload."""
+    from oracle import oracle_py as O
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    md = make_workload(args)
+    ub = md.unique_bytes()
+    cores = os.cpu_count()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    if O.ref_available():
+        kind = "reference"
+        for _ in range(max(0, min(args.warmup, 1))):
+            O.ref_omp(md, 1)
+        times = []
+        for _ in range(args.steps):
+            _, _, t_loop, _ = O.ref_omp(md, 1)
+            times.append(t_loop)
+        secs = sum(times) / len(times)
+        sample = "loopCPUCellCentredOMP, 1 iteration of the full mesh per step (colouring excluded)"
+    else:
+        kind = "port"
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            O.serial(md, 1)
+        secs = (time.perf_counter() - t0) / args.steps
+        cores = 1
+        sample = "oracle serial loop, 1 iteration of the full mesh per step"
+    v = ub / secs / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "faces": md.n_cells,
+                                            "cells": md.n_points[0], "unique_bytes_per_step": ub},
+            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="fot", choices=["fot", "reference"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plan", default=None, help="force a candidate label order/exec/block")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    rank, world, local = dist_setup(args.gpus)
+    from cuda_fot_b200 import fot as F
+    from cuda_fot_b200 import tune as T
+
+    md = make_workload(args)
+    ub = md.unique_bytes()
+    stream = torch.cuda.current_stream()
+
+    # plan choice: the cost model's pick when available, else the measured sweep
+    choice_src = "sweep"
+    chosen = None
+    try:
+        from cuda_fot_b200 import costmodel as CM
+        model = CM.load_default()
+        if model is not None:
+            chosen = CM.pick(model, md, T.default_candidates(md.loop))
+            choice_src = "cost model"
+    except Exception:
+        chosen = None
+    cache = T.OrderedCache(md)
+    sweep_res = []
+    if args.plan:
+        o, e, b = args.plan.split("/")
+        chosen = T.Candidate(None if o == "as-is" else o, 0, e, int(b))
+        choice_src = "forced"
+    if chosen is None:
+        for c in T.default_candidates(md.loop, quick=True):
+            sweep_res.append(T.measure(cache, c, iters=5, warmup=3))
+        chosen = T.best(sweep_res)["cand"]
+    atomic_plain = T.measure(cache, T.Candidate(None, 0, "atomic", 256), iters=10, warmup=3)
+
+    md_run = cache.get(chosen.order, chosen.partition)
+    p, plan = T.build(md_run, chosen)
+    launches_per_step = {"atomic": 1, "hier": 1}.get(chosen.exec, plan.stats()["n_colours"])
+
+    # ---- timed region: inputs resident in HBM -------------------------------
+    plan.run(args.warmup, stream)
+    p.sync(stream)
+    barrier(world)
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            plan.run(1, stream)
+        end.record(stream)
+        end.synchronize()
+    p.sync(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    secs = start.elapsed_time(end) / 1e3
+    secs_max = max_over_ranks(secs, world)
+    value = ub * args.steps * world / secs_max / 1e9
+    per_launch = secs / args.steps / launches_per_step
+
+    # ---- e2e: through the public API with host buffers ------------------------
+    host_in = []
+    for k in range(p.info.n_point_sets):
+        host_in.append(("p", k, torch.from_numpy(np.ascontiguousarray(md_run.point_data[k])).pin_memory()))
+    for j in range(p.info.n_cell_sets):
+        host_in.append(("c", j, torch.from_numpy(np.ascontiguousarray(md_run.cell_data[j])).pin_memory()))
+    host_out = torch.empty(md_run.point_data[0].shape, dtype=torch.float64).pin_memory()
+    h2d = sum(t.numel() * t.element_size() for _, _, t in host_in)
+    d2h = host_out.numel() * host_out.element_size()
+    e2e_steps = max(3, min(args.steps, 10))
+
+    def e2e_step():
+        for kind, k, t in host_in:
+            fn = F._lib.fot_set_point_data_async if kind == "p" else F._lib.fot_set_cell_data_async
+            F._check(fn(p._h, k, F.C.c_void_p(t.data_ptr()), F.C.c_size_t(t.numel() * t.element_size()),
+                        F._stream_ptr(stream)))
+        plan.run(1, stream)
+        F._check(F._lib.fot_get_point_data_async(p._h, 0, F.C.c_void_p(host_out.data_ptr()),
+                                                 F.C.c_size_t(d2h), F._stream_ptr(stream)))
+
+    e2e_step()
+    p.sync(stream)
+    barrier(world)
+    torch.cuda.synchronize()
+    s2 = torch.cuda.Event(enable_timing=True)
+    e2 = torch.cuda.Event(enable_timing=True)
+    s2.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2.record(stream)
+    e2.synchronize()
+    p.sync(stream)
+    e2e_secs = max_over_ranks(s2.elapsed_time(e2) / 1e3, world)
+    e2e_value = ub * e2e_steps * world / e2e_secs / 1e9
+
+    peak, peak_src = load_peaks()
+    achieved = ub / per_launch / 1e9 if launches_per_step == 1 else ub / (secs / args.steps) / 1e9
+    kernel_key = f"{chosen.exec}"
+    traffic = load_traffic(kernel_key)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(md)
+
+    if rank == 0:
+        st = plan.stats()
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs_max / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "faces": md.n_cells, "cells": md.n_points[0],
+                       "unique_bytes_per_step": ub, "seed": args.seed,
+                       "l2": "inputs larger than L2 (%.2f GB per step vs 126 MB L2)" % (ub / 1e9),
+                       "plan": chosen.label(), "plan_choice": choice_src,
+                       "n_blocks": st["n_blocks"], "block_colours": st["n_colours"],
+                       "parallelism": f"replicas x{world}"},
+            "atomic_baseline": {"plan": "as-is/atomic/256 (plain atomics on the random numbering)",
+                                "value": atomic_plain.get("gbs"), "unit": "GB/s"},
+            "speedup_vs_atomic": (value / world) / atomic_plain["gbs"] if atomic_plain.get("ok") else None,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_src,
+                         "traffic": traffic},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": args.steps * launches_per_step,
+            "clocks": clocks.summary(),
+        }
+        if sweep_res:
+            line["sweep"] = {r["cand"].label(): (round(r["gbs"], 1) if r["ok"] else None) for r in sweep_res}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

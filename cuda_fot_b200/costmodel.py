@@ -1,0 +1,308 @@
+"""The learned plan cost model.
+
+A 24 -> 64 -> 64 -> 1 MLP (libfot's fot_model_* kernels: forward, backward
+and Adam on the GPU) predicts log(seconds per iteration) of a candidate plan
+(ordering, partition, executor, block size; cuda_fot_b200.tune.Candidate) from
+features of the mesh AFTER the candidate's ordering and of the plan.  The
+autotuner's exhaustive measured sweep generates the training data and stays
+as the fallback and the judge: the model's pick is compared with the sweep's
+best (regret) and with a fixed default plan (what the model gains).
+
+Features (FEATURES below): mesh size and bytes, the loop kind, the histogram
+of point degrees, the bandwidth and mean cell span of the ordered mapping,
+and the plan descriptor.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+import time
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import fot as F
+from . import meshgen as mg
+from . import tune as T
+
+N_FEATURES = 24
+HERE = os.path.dirname(os.path.abspath(__file__))
+MODEL_DIR = os.path.join(HERE, "model")
+DEFAULT_MODEL = os.path.join(MODEL_DIR, "costmodel.npz")
+DEFAULT_CORPUS = os.path.join(MODEL_DIR, "corpus.npz")
+
+FEATURES = [
+    "log10_cells", "log10_points", "mesh_dim", "out_dim", "log10_unique_bytes",
+    "read_bytes_per_cell/100", "direct_bytes_per_cell/100",
+    "loop_res_calc", "loop_mini_aero", "loop_lulesh", "loop_volna", "loop_getacc",
+    "deg_le2", "deg_3_4", "deg_5_6", "deg_ge7",
+    "log10_1p_bandwidth", "log10_1p_mean_span",
+    "exec_atomic", "exec_hier", "exec_hier_launch", "log2_block", "partitioned", "direct_reads",
+]
+assert len(FEATURES) == N_FEATURES
+
+_lib = F._lib
+_fp = C.POINTER(C.c_float)
+
+
+def mesh_features(md: mg.MeshData) -> np.ndarray:
+    """17 features of a mesh in its current numbering."""
+    m0 = np.asarray(md.maps[0])
+    n, dim = m0.shape
+    np0 = md.n_points[0]
+    info = F.loop_info(md.loop)
+    read_bytes = 0
+    if md.loop == mg.RES_CALC:
+        read_bytes = dim * (2 * 8 + 4 * 8 + 8)
+    elif md.loop == mg.MINI_AERO:
+        read_bytes = dim * 28 * 8
+    elif md.loop == mg.LULESH:
+        read_bytes = dim * 3 * 8
+    elif md.loop == mg.VOLNA:
+        read_bytes = dim * 4
+    direct = sum(info.cell_dim[j] * info.cell_type_size[j] for j in range(info.n_cell_sets))
+    deg = np.bincount(m0.ravel(), minlength=np0)
+    hist = np.array([(deg <= 2).mean(), ((deg >= 3) & (deg <= 4)).mean(),
+                     ((deg >= 5) & (deg <= 6)).mean(), (deg >= 7).mean()])
+    span = (m0.max(axis=1).astype(np.int64) - m0.min(axis=1).astype(np.int64))
+    onehot = np.zeros(5)
+    onehot[md.loop] = 1
+    f = np.concatenate([
+        [np.log10(n), np.log10(np0), dim, info.point_dim[0], np.log10(md.unique_bytes()),
+         read_bytes / 100.0, direct / 100.0], onehot, hist,
+        [np.log10(1 + span.max()), np.log10(1 + span.mean())]])
+    return f.astype(np.float32)
+
+
+def plan_features(c: T.Candidate) -> np.ndarray:
+    ex = np.zeros(3)
+    ex[["atomic", "hier", "hier_launch"].index(c.exec)] = 1
+    return np.concatenate([ex, [np.log2(c.block), 1.0 if c.partition else 0.0,
+                                1.0 if (c.direct and c.exec != "atomic") else 0.0]]).astype(np.float32)
+
+
+def features(mesh_f: np.ndarray, c: T.Candidate) -> np.ndarray:
+    return np.concatenate([mesh_f, plan_features(c)]).astype(np.float32)
+
+
+# ---------------------------------------------------------------------------
+# the model (device kernels through the C ABI)
+# ---------------------------------------------------------------------------
+class CostModel:
+    def __init__(self, seed: int = 1):
+        self._h = C.c_void_p()
+        F._check(_lib.fot_model_create(C.c_uint64(seed), C.byref(self._h)))
+        self.n_params = _lib.fot_model_num_params()
+        self.mean = np.zeros(N_FEATURES, np.float32)
+        self.std = np.ones(N_FEATURES, np.float32)
+
+    def __del__(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.fot_model_destroy(self._h)
+            self._h = None
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.n_params, np.float32)
+        F._check(_lib.fot_model_get_params(self._h, p.ctypes.data_as(_fp)))
+        return p
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        F._check(_lib.fot_model_set_params(self._h, p.ctypes.data_as(_fp)))
+
+    def set_normalisation(self, mean: np.ndarray, std: np.ndarray) -> None:
+        self.mean = np.ascontiguousarray(mean, np.float32)
+        self.std = np.ascontiguousarray(std, np.float32)
+        F._check(_lib.fot_model_set_normalisation(self._h, self.mean.ctypes.data_as(_fp),
+                                                  self.std.ctypes.data_as(_fp)))
+
+    def predict(self, X: np.ndarray) -> np.ndarray:
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.zeros(X.shape[0], np.float32)
+        F._check(_lib.fot_model_predict(self._h, X.ctypes.data_as(_fp), X.shape[0], y.ctypes.data_as(_fp)))
+        return y
+
+    def grad(self, X: np.ndarray, t: np.ndarray):
+        X = np.ascontiguousarray(X, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        g = np.zeros(self.n_params, np.float32)
+        loss = C.c_float()
+        F._check(_lib.fot_model_grad(self._h, X.ctypes.data_as(_fp), t.ctypes.data_as(_fp), X.shape[0],
+                                     g.ctypes.data_as(_fp), C.byref(loss)))
+        return g, loss.value
+
+    def fit(self, X: np.ndarray, t: np.ndarray, epochs: int = 300, batch: int = 256,
+            lr: float = 2e-3, weight_decay: float = 1e-5, seed: int = 0) -> np.ndarray:
+        X = np.asarray(X, np.float32)
+        t = np.asarray(t, np.float32)
+        std = X.std(axis=0)
+        std[std < 1e-6] = 1.0
+        self.set_normalisation(X.mean(axis=0), std)
+        perm = np.random.default_rng(seed).permutation(X.shape[0])
+        Xs = np.ascontiguousarray(X[perm])
+        ts = np.ascontiguousarray(t[perm])
+        losses = np.zeros(epochs, np.float32)
+        F._check(_lib.fot_model_train(self._h, Xs.ctypes.data_as(_fp), ts.ctypes.data_as(_fp),
+                                      Xs.shape[0], epochs, batch, C.c_float(lr),
+                                      C.c_float(weight_decay), losses.ctypes.data_as(_fp)))
+        return losses
+
+    def save(self, path: str) -> None:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        np.savez(path, params=self.params(), mean=self.mean, std=self.std,
+                 features=np.array(FEATURES))
+
+    @classmethod
+    def load(cls, path: str) -> "CostModel":
+        z = np.load(path)
+        m = cls()
+        m.set_params(z["params"])
+        m.set_normalisation(z["mean"], z["std"])
+        return m
+
+
+def load_default() -> Optional[CostModel]:
+    if os.path.exists(DEFAULT_MODEL):
+        return CostModel.load(DEFAULT_MODEL)
+    return None
+
+
+# ---------------------------------------------------------------------------
+# training data: measured sweeps over seeded synthetic meshes
+# ---------------------------------------------------------------------------
+def corpus_candidates(loop: int) -> List[T.Candidate]:
+    """Plan candidates of one (mesh, ordering): executors x block sizes x
+    staging; partitioned variants are separate orderings."""
+    out = [T.Candidate(None, 0, "atomic", 256)]
+    for b in (64, 128, 256, 512):
+        out.append(T.Candidate(None, 0, "hier", b, False))
+        out.append(T.Candidate(None, 0, "hier", b, True))
+    out.append(T.Candidate(None, 0, "hier_launch", 256, False))
+    out.append(T.Candidate(None, 0, "hier_launch", 256, True))
+    return out
+
+
+ORDERINGS = [(None, 0), ("random", 0), ("rcm", 0), ("gps", 0), ("gps", 128), ("gps", 256),
+             ("rcm", 256), ("gps", 512)]
+
+
+def mesh_for(loop: int, cells: float, seed: int) -> mg.MeshData:
+    """A seeded mesh of about `cells` elements of the given loop."""
+    if loop == mg.RES_CALC:
+        n = max(8, int(round(np.sqrt(cells / 2))))
+        return mg.res_calc(n, n, seed)
+    if loop == mg.MINI_AERO:
+        n = max(4, int(round((cells / 3) ** (1 / 3))))
+        return mg.mini_aero(n, seed, permute=True)
+    if loop == mg.LULESH:
+        n = max(4, int(round(cells ** (1 / 3))))
+        return mg.lulesh(n, seed, permute=True)
+    if loop == mg.VOLNA:
+        n = max(8, int(round(np.sqrt(cells / 3))))
+        return mg.volna(n, n, seed)
+    n = max(8, int(round(np.sqrt(cells))))
+    return mg.getacc(n, n, seed)
+
+
+def generate(loops: Sequence[int], sizes: Sequence[float], seeds: Sequence[int],
+             out_path: str = DEFAULT_CORPUS, iters_min_ms: float = 2.0, verbose: bool = True,
+             time_limit_s: float = 1e9) -> dict:
+    """Time every (mesh, ordering, plan) and store features and log times."""
+    X, y, group, labels, secs_all = [], [], [], [], []
+    info = []
+    t_start = time.time()
+    gid = 0
+    for seed in seeds:
+        for loop in loops:
+            for size in sizes:
+                if time.time() - t_start > time_limit_s:
+                    break
+                md = mesh_for(loop, size, seed)
+                cache = T.OrderedCache(md)
+                for order, part in ORDERINGS:
+                    t_o = time.time()
+                    mdo = cache.get(order, part)
+                    order_s = time.time() - t_o
+                    mf = mesh_features(mdo)
+                    for c in corpus_candidates(loop):
+                        if part:
+                            # blocks follow the parts: block size = part size
+                            blk = 256 if c.exec == "atomic" else part
+                            if c.exec != "atomic" and c.block != 256:
+                                continue
+                            c = T.Candidate(order, part, c.exec, blk, c.direct)
+                        else:
+                            c = T.Candidate(order, 0, c.exec, c.block, c.direct)
+                        try:
+                            p, plan = T.build(mdo, c)
+                            t1 = T.time_plan(p, plan, iters=2, warmup=1)
+                            iters = int(min(50, max(3, iters_min_ms * 1e-3 / max(t1, 1e-7))))
+                            secs = T.time_plan(p, plan, iters=iters, warmup=1)
+                            del plan, p
+                        except F.FotError:
+                            continue
+                        X.append(features(mf, c))
+                        y.append(np.log(secs))
+                        secs_all.append(secs)
+                        group.append(gid)
+                        labels.append(c.label())
+                    if verbose:
+                        print(f"  {mg.LOOP_NAMES[loop]} {md.n_cells} seed {seed} {order}+{part}: "
+                              f"{len(y)} samples, order {order_s:.2f}s, total {time.time()-t_start:.0f}s",
+                              flush=True)
+                info.append({"gid": gid, "loop": loop, "cells": md.n_cells, "seed": seed})
+                gid += 1
+                del cache
+    data = {"X": np.array(X, np.float32), "y": np.array(y, np.float32),
+            "seconds": np.array(secs_all, np.float64), "group": np.array(group, np.int32),
+            "label": np.array(labels), "info": json.dumps(info)}
+    if out_path:
+        os.makedirs(os.path.dirname(out_path), exist_ok=True)
+        np.savez_compressed(out_path, **data)
+    return data
+
+
+def load_corpus(path: str = DEFAULT_CORPUS) -> dict:
+    z = np.load(path, allow_pickle=False)
+    return {k: z[k] for k in z.files}
+
+
+DEFAULT_PLAN = "gps/atomic/256"  # the method without the model: a fixed default
+
+
+def evaluate(model: CostModel, data: dict, mask: np.ndarray) -> dict:
+    """Regret of the model's pick vs the measured best per mesh group, and the
+    default plan's regret, over the rows selected by mask."""
+    X = data["X"][mask]
+    secs = data["seconds"][mask]
+    groups = data["group"][mask]
+    labels = data["label"][mask]
+    pred = model.predict(X)
+    regrets, default_regrets, picks = [], [], []
+    for g in np.unique(groups):
+        idx = np.where(groups == g)[0]
+        best = secs[idx].min()
+        pick = idx[np.argmin(pred[idx])]
+        regrets.append(secs[pick] / best - 1.0)
+        d = [i for i in idx if labels[i] == DEFAULT_PLAN]
+        if d:
+            default_regrets.append(secs[d[0]] / best - 1.0)
+        picks.append(str(labels[pick]))
+    return {"groups": int(len(regrets)), "mean_regret": float(np.mean(regrets)),
+            "median_regret": float(np.median(regrets)), "max_regret": float(np.max(regrets)),
+            "default_mean_regret": float(np.mean(default_regrets)) if default_regrets else None,
+            "picks": picks}
+
+
+def pick(model: CostModel, md: mg.MeshData, candidates: List[T.Candidate]) -> T.Candidate:
+    """The candidate with the smallest predicted time (orderings are applied
+    to compute the ordered-mesh features)."""
+    cache = T.OrderedCache(md)
+    rows, cands = [], []
+    for c in candidates:
+        mf = mesh_features(cache.get(c.order, c.partition))
+        rows.append(features(mf, c))
+        cands.append(c)
+    pred = model.predict(np.array(rows))
+    return cands[int(np.argmin(pred))]

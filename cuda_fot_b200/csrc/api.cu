@@ -147,6 +147,7 @@ fot::HierPlanDev fot_plan::dev(uint32_t iterations) const {
   P.total_tiles = iterations * n_blocks;
   for (int r = 0; r < 4; ++r) P.read_off[r] = read_off[r];
   P.acc_off = acc_off;
+  P.pts_smem_off = pts_smem_off;
   P.ctl = ctl.as<Ctl>();
   return P;
 }
@@ -359,12 +360,14 @@ int fot_plan_build(fot_problem *p, const fot_plan_desc *desc, fot_plan **out) {
   int rc = FOT_OK;
   if (desc->exec == FOT_EXEC_ATOMIC) {
     plan->threads = 256;
-    rc = ops->occupancy(FOT_EXEC_ATOMIC, p->layout == FOT_SOA, 256, 0, &plan->per_sm);
+    rc = ops->occupancy(FOT_EXEC_ATOMIC, p->layout == FOT_SOA, 256, 0, 0, &plan->per_sm);
   } else if (desc->exec == FOT_EXEC_HIER || desc->exec == FOT_EXEC_HIER_LAUNCH) {
+    plan->variant = (desc->flags & FOT_PLAN_DIRECT_READS) ? 0u : 1u;
     rc = build_hier_plan(p, plan);
     if (rc == FOT_OK) {
       plan->threads = hier_threads(desc->block_size);
-      plan->smem = ops->smem_layout(plan->cap[0], plan->cap[1], plan->read_off, &plan->acc_off);
+      plan->smem = ops->smem_layout(plan->cap[0], plan->cap[1], plan->variant, plan->read_off,
+                                    &plan->pts_smem_off, &plan->acc_off);
       if (plan->smem > 227 * 1024)
         rc = fail(FOT_ERR_LIMIT,
                   "a block needs %zu bytes of shared memory (limit 227 KB): use a smaller block "
@@ -372,8 +375,8 @@ int fot_plan_build(fot_problem *p, const fot_plan_desc *desc, fot_plan **out) {
                   plan->smem);
     }
     if (rc == FOT_OK)
-      rc = ops->occupancy(desc->exec, p->layout == FOT_SOA, plan->threads, plan->smem,
-                          &plan->per_sm);
+      rc = ops->occupancy(desc->exec, p->layout == FOT_SOA, plan->threads, plan->variant,
+                          plan->smem, &plan->per_sm);
     if (rc == FOT_OK && plan->per_sm == 0)
       rc = fail(FOT_ERR_LIMIT, "hierarchical kernel cannot be resident (%zu B smem, %u threads)",
                 plan->smem, plan->threads);
@@ -470,14 +473,16 @@ static int run_plan(fot_problem *p, fot_plan *plan, uint32_t iterations, cudaStr
       return fail(FOT_ERR_LIMIT, "too many tiles in one launch");
     const HierPlanDev P = plan->dev(iterations);
     const uint32_t grid = std::min<uint32_t>(P.total_tiles, (uint32_t)(plan->per_sm * sms));
-    return ops->run_hier(d, P, soa, plan->threads, grid, plan->smem, st);
+    return ops->run_hier(d, P, soa, plan->threads, plan->variant, grid, plan->smem, st);
   }
   const HierPlanDev P = plan->dev(1);
   for (uint32_t it = 0; it < iterations; ++it)
     for (uint32_t c = 0; c < plan->n_colours; ++c) {
       const uint32_t first = plan->colour_offsets[c];
       const uint32_t count = plan->colour_offsets[c + 1] - first;
-      if (count) FOT_TRY(ops->run_hier_colour(d, P, soa, plan->threads, first, count, plan->smem, st));
+      if (count)
+        FOT_TRY(ops->run_hier_colour(d, P, soa, plan->threads, plan->variant, first, count,
+                                     plan->smem, st));
     }
   return FOT_OK;
 }

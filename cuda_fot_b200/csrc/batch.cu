@@ -34,9 +34,8 @@ struct BatchDev {
 template <bool SOA, int T, class L>
 __device__ __forceinline__ void batch_tile(const BatchMesh &m, unsigned char *smem, uint32_t b,
                                            uint32_t iter, unsigned int *done, unsigned int *err) {
-  int abort = 0;
-  hier_tile<L, SOA, T, true>(m.d, m.P, smem, b, iter * m.P.n_blocks + m.P.block_wait[b], done,
-                             err, abort);
+  unsigned int seen = 0;  // counters differ per mesh: no cached value
+  hier_tile_waiting<L, SOA, T>(m.d, m.P, smem, b, iter, done, err, seen);
 }
 
 template <bool SOA, int T, class... Ls>
@@ -61,10 +60,7 @@ __global__ void __launch_bounds__(T) k_batch(BatchDev B) {
     ((m.loop == Ls::kLoop ? (batch_tile<SOA, T, Ls>(m, smem, b, iter, &B.done[mi], &B.ctl->error), 0)
                           : 0),
      ...);
-    if (tid == 0) {
-      __threadfence();
-      atomicAdd(&B.done[mi], 1u);
-    }
+    if (tid == 0) red_release_add(&B.done[mi], 1u);
   }
   if (tid == 0) {
     __threadfence();

@@ -13,23 +13,27 @@
 namespace fot {
 
 // Per-loop entry points, one table per loop translation unit (loop_*.cu).
+// `variant` selects the hierarchical tile kernel: bit 0 = stage the read rows
+// in shared memory (else gather them straight from HBM/L2).
 struct LoopOps {
   // launch one iteration of the atomic executor
   int (*run_atomic)(const LoopData &d, bool soa, bool aggregate, uint32_t threads,
                     uint32_t grid, cudaStream_t st);
   // persistent hierarchical launch over P.total_tiles tiles
   int (*run_hier)(const LoopData &d, const HierPlanDev &P, bool soa, uint32_t threads,
-                  uint32_t grid, size_t smem, cudaStream_t st);
+                  uint32_t variant, uint32_t grid, size_t smem, cudaStream_t st);
   // one launch per block colour: blocks [first, first + count)
   int (*run_hier_colour)(const LoopData &d, const HierPlanDev &P, bool soa,
-                         uint32_t threads, uint32_t first, uint32_t count, size_t smem,
-                         cudaStream_t st);
+                         uint32_t threads, uint32_t variant, uint32_t first, uint32_t count,
+                         size_t smem, cudaStream_t st);
   // resident CTAs per SM of an executor configuration (0 if it cannot launch)
-  int (*occupancy)(int exec, bool soa, uint32_t threads, size_t smem, int *per_sm);
-  // shared-memory layout of a hierarchical tile: byte offsets of the read
-  // sets and of the accumulator for at most cap0 / cap1 points per block
-  size_t (*smem_layout)(uint32_t cap0, uint32_t cap1, uint32_t read_off[4],
-                        uint32_t *acc_off);
+  int (*occupancy)(int exec, bool soa, uint32_t threads, uint32_t variant, size_t smem,
+                   int *per_sm);
+  // shared-memory layout of a hierarchical tile for at most cap0 / cap1
+  // points per block: byte offsets of the read sets, the point lists and the
+  // accumulator; returns the bytes per CTA
+  size_t (*smem_layout)(uint32_t cap0, uint32_t cap1, uint32_t variant, uint32_t read_off[4],
+                        uint32_t *pts_off, uint32_t *acc_off);
 };
 
 const LoopOps *loop_ops(int loop);
@@ -84,6 +88,7 @@ struct fot_plan {
   uint64_t version = 0;
   fot_plan_desc desc{};
   fot_plan_stats stats{};
+  uint32_t variant = 0; // hierarchical tile kernel variant (see LoopOps)
   // hierarchical plans
   uint32_t n_blocks = 0, n_colours = 0;
   std::vector<uint32_t> colour_offsets; // host copy (n_colours + 1)
@@ -93,6 +98,7 @@ struct fot_plan {
   uint32_t cap[2] = {0, 0};
   uint32_t read_off[4] = {0, 0, 0, 0};
   uint32_t acc_off = 0;
+  uint32_t pts_smem_off = 0;
   size_t smem = 0;
   uint32_t threads = 0;
   int per_sm = 0;

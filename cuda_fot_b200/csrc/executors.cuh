@@ -55,6 +55,7 @@ struct HierPlanDev {
   uint32_t total_tiles;        // iterations * n_blocks (persistent form)
   uint32_t read_off[4];        // shared-memory byte offset of each read set
   uint32_t acc_off;            // shared-memory byte offset of the accumulator
+  uint32_t pts_smem_off;       // shared-memory byte offset of the tile's point lists
   Ctl *ctl;
 };
 
@@ -139,7 +140,8 @@ __device__ __forceinline__ void load_row(const uint32_t *__restrict__ map, uint3
 template <class T> __device__ __forceinline__ void atomic_add(T *a, T v) { atomicAdd(a, v); }
 
 template <class L, bool SOA, bool AGG>
-__global__ void __launch_bounds__(256) k_atomic(LoopData d) {
+__global__ void __launch_bounds__(256, (65536 / (256 * L::kRegCap)) > 0 ? 65536 / (256 * L::kRegCap) : 1)
+    k_atomic(LoopData d) {
   using out_t = typename L::out_t;
   constexpr int D = L::kDim, K = L::kOut;
   const uint32_t lane = threadIdx.x & 31u;
@@ -205,213 +207,6 @@ __global__ void __launch_bounds__(256) k_atomic(LoopData d) {
   }
 }
 
-// ===========================================================================
-// (b) hierarchical executor
-// ===========================================================================
-
-// One tile: block b of plan P.  With WAIT, the write-back first waits until
-// *done >= wait_target (bounded; on timeout *err gets kErrWaitLimit and the
-// tile skips its write-back).
-template <class L, bool SOA, int THREADS, bool WAIT>
-__device__ __forceinline__ void hier_tile(const LoopData &d, const HierPlanDev &P,
-                                          unsigned char *smem, uint32_t b,
-                                          uint32_t wait_target, unsigned int *done,
-                                          unsigned int *err, int &abort) {
-  using out_t = typename L::out_t;
-  using read_t = typename L::read_t;
-  constexpr int D = L::kDim, K = L::kOut;
-  const uint32_t tid = threadIdx.x;
-  const uint32_t start = P.block_start[b];
-  const uint32_t ncell = P.block_start[b + 1] - start;
-  const uint32_t off0 = P.pts_off[0][b];
-  const uint32_t n0 = P.pts_off[0][b + 1] - off0;
-  const uint32_t *__restrict__ pts0 = P.pts[0] + off0;
-  uint32_t off1 = 0, n1 = 0;
-  const uint32_t *__restrict__ pts1 = nullptr;
-  if constexpr (L::kHasClass1) {
-    off1 = P.pts_off[1][b];
-    n1 = P.pts_off[1][b + 1] - off1;
-    pts1 = P.pts[1] + off1;
-  }
-  const uint32_t ntcol = P.block_ntcol[b];
-
-  // 1. stage the read rows of the block's unique points (cp.async)
-  static_for_read<L>([&](auto r) {
-    constexpr int R = decltype(r)::value;
-    constexpr int DIM = L::read_dim(R);
-    constexpr int ROW = DIM * (int)sizeof(read_t);
-    const uint32_t n = L::read_class(R) == 0 ? n0 : n1;
-    const uint32_t *__restrict__ pts = L::read_class(R) == 0 ? pts0 : pts1;
-    const char *src = static_cast<const char *>(d.point[L::read_set(R)]);
-    char *dst = reinterpret_cast<char *>(smem + P.read_off[R]);
-    if constexpr (!SOA) {
-      if constexpr (ROW % 16 == 0) {
-        constexpr int CH = ROW / 16;
-        for (uint32_t e = tid; e < n * CH; e += THREADS) {
-          const uint32_t i = e / CH, c = e - i * CH;
-          cp_async16(dst + (size_t)i * ROW + c * 16, src + (size_t)pts[i] * ROW + c * 16);
-        }
-      } else if constexpr (ROW % 8 == 0) {
-        constexpr int CH = ROW / 8;
-        for (uint32_t e = tid; e < n * CH; e += THREADS) {
-          const uint32_t i = e / CH, c = e - i * CH;
-          cp_async8(dst + (size_t)i * ROW + c * 8, src + (size_t)pts[i] * ROW + c * 8);
-        }
-      } else {
-        constexpr int CH = ROW / 4;
-        for (uint32_t e = tid; e < n * CH; e += THREADS) {
-          const uint32_t i = e / CH, c = e - i * CH;
-          cp_async4(dst + (size_t)i * ROW + c * 4, src + (size_t)pts[i] * ROW + c * 4);
-        }
-      }
-    } else {
-      const uint32_t np = d.n_points[L::read_set(R)];
-      for (uint32_t e = tid; e < n * DIM; e += THREADS) {
-        const uint32_t k = e / n, i = e - k * n;
-        const char *g = src + ((size_t)k * np + pts[i]) * sizeof(read_t);
-        char *s = dst + ((size_t)i * DIM + k) * sizeof(read_t);
-        if constexpr (sizeof(read_t) == 8) cp_async8(s, g);
-        else cp_async4(s, g);
-      }
-    }
-  });
-  // 2. zero the accumulator while the copies fly
-  out_t *acc = reinterpret_cast<out_t *>(smem + P.acc_off);
-  for (uint32_t e = tid; e < n0 * K; e += THREADS) acc[e] = out_t(0);
-  // 3. per-cell local indices and thread colour (coalesced loads)
-  const bool active = tid < ncell;
-  const uint32_t pos = start + tid;
-  SmemRows<L> rows;
-  uint32_t my_col = 0xFFFFFFFFu;
-  if (active) {
-#pragma unroll
-    for (int s = 0; s < D; ++s) {
-      rows.l[0][s] = P.lidx[0][(size_t)s * d.n_cells + pos];
-      rows.l[1][s] = L::kHasClass1 ? P.lidx[1][(size_t)s * d.n_cells + pos] : 0;
-    }
-    my_col = P.tcol[pos];
-  }
-  static_for_read<L>([&](auto r) {
-    constexpr int R = decltype(r)::value;
-    rows.base[R] = reinterpret_cast<const read_t *>(smem + P.read_off[R]);
-  });
-  cp_async_wait_all();
-  __syncthreads();
-  // 4. compute
-  out_t inc[D][K];
-  if (active) {
-    Direct dir{d.cell, pos, d.n_cells};
-    L::cell(rows, dir, inc);
-  }
-  // 5. accumulate in thread-colour order
-  for (uint32_t col = 0; col < ntcol; ++col) {
-    if (my_col == col) {
-#pragma unroll
-      for (int s = 0; s < D; ++s)
-#pragma unroll
-        for (int k = 0; k < K; ++k) acc[(uint32_t)rows.l[0][s] * K + k] += inc[s][k];
-    }
-    __syncthreads();
-  }
-  // 6. wait until every tile of the earlier colours has written back
-  if constexpr (WAIT) {
-    __shared__ int s_abort;
-    if (tid == 0) {
-      unsigned int polls = 0;
-      int ab = 0;
-      while (ld_acquire_gpu(done) < wait_target) {
-        if (++polls > kWaitPollLimit) {
-          atomicOr(err, kErrWaitLimit);
-          ab = 1;
-          break;
-        }
-        __nanosleep(256);
-      }
-      s_abort = ab;
-    }
-    __syncthreads();
-    abort = s_abort;
-  }
-  // 7. write back: out[p] += acc (L2 loads/stores; L1 may hold stale lines)
-  if (!abort) {
-    out_t *__restrict__ out = static_cast<out_t *>(d.out);
-    if constexpr (!SOA && (K * sizeof(out_t)) % 16 == 0) {
-      constexpr int CH = K * sizeof(out_t) / 16;
-      using vec_t = typename std::conditional<sizeof(out_t) == 8, double2, float4>::type;
-      vec_t *o = reinterpret_cast<vec_t *>(out);
-      const vec_t *a = reinterpret_cast<const vec_t *>(acc);
-      for (uint32_t e = tid; e < n0 * CH; e += THREADS) {
-        const uint32_t i = e / CH, c = e - i * CH;
-        const size_t gi = (size_t)pts0[i] * CH + c;
-        vec_t v = __ldcg(o + gi);
-        const vec_t w = a[e];
-        if constexpr (sizeof(out_t) == 8) {
-          v.x += w.x;
-          v.y += w.y;
-        } else {
-          v.x += w.x;
-          v.y += w.y;
-          v.z += w.z;
-          v.w += w.w;
-        }
-        __stcg(o + gi, v);
-      }
-    } else {
-      for (uint32_t e = tid; e < n0 * K; e += THREADS) {
-        const uint32_t i = e / K, k = e - i * K;
-        const size_t gi = out_index(SOA, d.n_points[0], pts0[i], K, k);
-        __stcg(out + gi, __ldcg(out + gi) + acc[e]);
-      }
-    }
-  }
-  __syncthreads();
-}
-
-// Persistent form: CTAs claim tiles in colour order until the queue is empty.
-template <class L, bool SOA, int THREADS>
-__global__ void __launch_bounds__(THREADS) k_hier(LoopData d, HierPlanDev P) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ uint32_t s_ticket;
-  const uint32_t tid = threadIdx.x;
-  for (;;) {
-    if (tid == 0) {
-      uint32_t t = atomicAdd(&P.ctl->ticket, 1u);
-      if (*(volatile unsigned int *)&P.ctl->error) t = P.total_tiles;
-      s_ticket = t;
-    }
-    __syncthreads();
-    const uint32_t t = s_ticket;
-    if (t >= P.total_tiles) break;
-    const uint32_t iter = t / P.n_blocks;
-    const uint32_t b = t - iter * P.n_blocks;
-    int abort = 0;
-    hier_tile<L, SOA, THREADS, true>(d, P, smem, b, iter * P.n_blocks + P.block_wait[b],
-                                     &P.ctl->done, &P.ctl->error, abort);
-    if (tid == 0) {
-      __threadfence();
-      atomicAdd(&P.ctl->done, 1u);
-    }
-  }
-  // the last CTA to leave resets the queue for the next launch
-  if (tid == 0) {
-    __threadfence();
-    const unsigned int prev = atomicAdd(&P.ctl->exited, 1u);
-    if (prev == gridDim.x - 1) {
-      atomicExch(&P.ctl->ticket, 0u);
-      atomicExch(&P.ctl->done, 0u);
-      atomicExch(&P.ctl->exited, 0u);
-      __threadfence();
-    }
-  }
-}
-
-// One launch per block colour: CTA x handles block first + x, no waiting.
-template <class L, bool SOA, int THREADS>
-__global__ void __launch_bounds__(THREADS) k_hier_colour(LoopData d, HierPlanDev P,
-                                                         uint32_t first) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  int abort = 0;
-  hier_tile<L, SOA, THREADS, false>(d, P, smem, first + blockIdx.x, 0, nullptr, nullptr, abort);
-}
-
 } // namespace fot
+
+#include "hier.cuh"

@@ -26,27 +26,32 @@ int run_atomic(const LoopData &d, bool soa, bool agg, uint32_t threads, uint32_t
              : launch_atomic<false, false>(d, threads, grid, st);
 }
 
-template <bool SOA, int T> const void *hier_kernel(bool persistent) {
-  return persistent ? reinterpret_cast<const void *>(&k_hier<L, SOA, T>)
-                    : reinterpret_cast<const void *>(&k_hier_colour<L, SOA, T>);
+template <bool SOA, int T, bool STAGE> const void *hier_kernel(bool persistent) {
+  return persistent ? reinterpret_cast<const void *>(&k_hier<L, SOA, T, STAGE>)
+                    : reinterpret_cast<const void *>(&k_hier_colour<L, SOA, T, STAGE>);
 }
 
-template <bool SOA> const void *hier_kernel_t(bool persistent, uint32_t threads) {
+template <bool SOA, bool STAGE> const void *hier_kernel_t(bool persistent, uint32_t threads) {
   switch (threads) {
-  case 128: return hier_kernel<SOA, 128>(persistent);
-  case 256: return hier_kernel<SOA, 256>(persistent);
-  case 512: return hier_kernel<SOA, 512>(persistent);
-  case 1024: return hier_kernel<SOA, 1024>(persistent);
+  case 128: return hier_kernel<SOA, 128, STAGE>(persistent);
+  case 256: return hier_kernel<SOA, 256, STAGE>(persistent);
+  case 512: return hier_kernel<SOA, 512, STAGE>(persistent);
+  case 1024: return hier_kernel<SOA, 1024, STAGE>(persistent);
   }
   return nullptr;
 }
 
-const void *kernel_for(int exec, bool soa, uint32_t threads) {
+// variant bit 0: staged reads
+const void *kernel_for(int exec, bool soa, uint32_t threads, uint32_t variant) {
   if (exec == FOT_EXEC_ATOMIC)
     return soa ? reinterpret_cast<const void *>(&k_atomic<L, true, true>)
                : reinterpret_cast<const void *>(&k_atomic<L, false, true>);
   const bool persistent = exec == FOT_EXEC_HIER;
-  return soa ? hier_kernel_t<true>(persistent, threads) : hier_kernel_t<false>(persistent, threads);
+  const bool stage = variant & 1u;
+  if (soa) return stage ? hier_kernel_t<true, true>(persistent, threads)
+                        : hier_kernel_t<true, false>(persistent, threads);
+  return stage ? hier_kernel_t<false, true>(persistent, threads)
+               : hier_kernel_t<false, false>(persistent, threads);
 }
 
 int prepare(const void *k, size_t smem) {
@@ -55,8 +60,8 @@ int prepare(const void *k, size_t smem) {
 }
 
 int run_hier(const LoopData &d, const HierPlanDev &P, bool soa, uint32_t threads,
-             uint32_t grid, size_t smem, cudaStream_t st) {
-  const void *k = kernel_for(FOT_EXEC_HIER, soa, threads);
+             uint32_t variant, uint32_t grid, size_t smem, cudaStream_t st) {
+  const void *k = kernel_for(FOT_EXEC_HIER, soa, threads, variant);
   if (!k) return fail(FOT_ERR_ARG, "no hierarchical kernel for %u threads", threads);
   FOT_TRY(prepare(k, smem));
   void *args[] = {const_cast<LoopData *>(&d), const_cast<HierPlanDev *>(&P)};
@@ -65,8 +70,9 @@ int run_hier(const LoopData &d, const HierPlanDev &P, bool soa, uint32_t threads
 }
 
 int run_hier_colour(const LoopData &d, const HierPlanDev &P, bool soa, uint32_t threads,
-                    uint32_t first, uint32_t count, size_t smem, cudaStream_t st) {
-  const void *k = kernel_for(FOT_EXEC_HIER_LAUNCH, soa, threads);
+                    uint32_t variant, uint32_t first, uint32_t count, size_t smem,
+                    cudaStream_t st) {
+  const void *k = kernel_for(FOT_EXEC_HIER_LAUNCH, soa, threads, variant);
   if (!k) return fail(FOT_ERR_ARG, "no hierarchical kernel for %u threads", threads);
   FOT_TRY(prepare(k, smem));
   void *args[] = {const_cast<LoopData *>(&d), const_cast<HierPlanDev *>(&P), &first};
@@ -74,8 +80,8 @@ int run_hier_colour(const LoopData &d, const HierPlanDev &P, bool soa, uint32_t 
   return FOT_OK;
 }
 
-int occupancy(int exec, bool soa, uint32_t threads, size_t smem, int *per_sm) {
-  const void *k = kernel_for(exec, soa, exec == FOT_EXEC_ATOMIC ? 256 : threads);
+int occupancy(int exec, bool soa, uint32_t threads, uint32_t variant, size_t smem, int *per_sm) {
+  const void *k = kernel_for(exec, soa, exec == FOT_EXEC_ATOMIC ? 256 : threads, variant);
   if (!k) return fail(FOT_ERR_ARG, "no kernel for %u threads", threads);
   if (exec != FOT_EXEC_ATOMIC) FOT_TRY(prepare(k, smem));
   FOT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
@@ -83,17 +89,24 @@ int occupancy(int exec, bool soa, uint32_t threads, size_t smem, int *per_sm) {
   return FOT_OK;
 }
 
-size_t smem_layout(uint32_t cap0, uint32_t cap1, uint32_t read_off[4], uint32_t *acc_off) {
+size_t smem_layout(uint32_t cap0, uint32_t cap1, uint32_t variant, uint32_t read_off[4],
+                   uint32_t *pts_off, uint32_t *acc_off) {
+  const bool stage = variant & 1u;
   size_t off = 0;
   for (int r = 0; r < 4; ++r) read_off[r] = 0;
-  for (int r = 0; r < L::kNumRead; ++r) {
-    read_off[r] = (uint32_t)off;
-    const uint32_t cap = L::read_class(r) == 0 ? cap0 : cap1;
-    off += (size_t)cap * L::read_dim(r) * sizeof(typename L::read_t);
-    off = (off + 15) & ~size_t(15);
+  if (stage) {
+    for (int r = 0; r < L::kNumRead; ++r) {
+      read_off[r] = (uint32_t)off;
+      const uint32_t cap = L::read_class(r) == 0 ? cap0 : cap1;
+      off += (size_t)cap * L::read_dim(r) * sizeof(typename L::read_t);
+      off = (off + 15) & ~size_t(15);
+    }
   }
   *acc_off = (uint32_t)off;
   off += (size_t)cap0 * L::kOut * sizeof(typename L::out_t);
+  off = (off + 15) & ~size_t(15);
+  *pts_off = (uint32_t)off;
+  off += (size_t)(cap0 + (stage && L::kHasClass1 ? cap1 : 0)) * sizeof(uint32_t);
   return (off + 15) & ~size_t(15);
 }
 

@@ -65,6 +65,7 @@ struct Loop {
   using read_t = double;
   static constexpr int kNumRead = 3;
   static constexpr bool kHasClass1 = true;
+  static constexpr int kRegCap = 64; // registers per thread the tile kernels are held to
   // read set r: x (set 1, class 1, dim 2), q (set 2, class 0, dim 4), adt (set 3, class 0, dim 1)
   __host__ __device__ static constexpr int read_set(int r) { return r + 1; }
   __host__ __device__ static constexpr int read_class(int r) { return r == 0 ? 1 : 0; }
@@ -101,6 +102,7 @@ struct Loop {
   using read_t = double;
   static constexpr int kNumRead = 1;
   static constexpr bool kHasClass1 = false;
+  static constexpr int kRegCap = 128; // registers per thread the tile kernels are held to
   __host__ __device__ static constexpr int read_set(int) { return 1; }
   __host__ __device__ static constexpr int read_class(int) { return 0; }
   __host__ __device__ static constexpr int read_dim(int) { return 28; }
@@ -147,6 +149,7 @@ struct Loop {
   using read_t = double;
   static constexpr int kNumRead = 1;
   static constexpr bool kHasClass1 = false;
+  static constexpr int kRegCap = 96; // registers per thread the tile kernels are held to
   __host__ __device__ static constexpr int read_set(int) { return 1; }
   __host__ __device__ static constexpr int read_class(int) { return 0; }
   __host__ __device__ static constexpr int read_dim(int) { return 3; }
@@ -191,6 +194,7 @@ struct Loop {
   using read_t = float;
   static constexpr int kNumRead = 1;
   static constexpr bool kHasClass1 = false;
+  static constexpr int kRegCap = 64; // registers per thread the tile kernels are held to
   __host__ __device__ static constexpr int read_set(int) { return 1; }
   __host__ __device__ static constexpr int read_class(int) { return 0; }
   __host__ __device__ static constexpr int read_dim(int) { return 1; }
@@ -229,6 +233,7 @@ struct Loop {
   using read_t = double;
   static constexpr int kNumRead = 0;
   static constexpr bool kHasClass1 = false;
+  static constexpr int kRegCap = 96; // registers per thread the tile kernels are held to
   __host__ __device__ static constexpr int read_set(int) { return 0; }
   __host__ __device__ static constexpr int read_class(int) { return 0; }
   __host__ __device__ static constexpr int read_dim(int) { return 1; }

@@ -1,0 +1,157 @@
+"""Autotuner: candidate plans and their measured timings.
+
+A candidate is (ordering, partition size, executor, block size):
+
+* ordering  -- None (keep the numbering), "natural" (cells sorted by point
+  tuple), "random", "rcm" or "gps" (fot_reorder);
+* partition -- 0, or the part size of fot_partition followed by
+  fot_reorder_to_partition and fot_renumber_points (the reference's
+  partition -> reorderToPartition -> renumberPoints sequence);
+* executor  -- "atomic", "hier" (persistent) or "hier_launch";
+* block     -- cells per block (hierarchical) / threads per CTA (atomic).
+
+``measure(md, cand)`` builds the candidate on a fresh problem and times
+``iters`` iterations with CUDA events on the launching stream after warm-up.
+The exhaustive sweep over a candidate list is the fallback and the judge of
+the learned cost model (cuda_fot_b200/costmodel.py), and it produces that
+model's training data.
+"""
+from __future__ import annotations
+
+import itertools
+import time
+from dataclasses import asdict, dataclass
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from . import fot as F
+from . import meshgen as mg
+
+ORDERS = {None: None, "natural": F.ORDER_NATURAL, "random": F.ORDER_RANDOM,
+          "rcm": F.ORDER_RCM, "gps": F.ORDER_GPS}
+EXECS = {"atomic": F.EXEC_ATOMIC, "hier": F.EXEC_HIER, "hier_launch": F.EXEC_HIER_LAUNCH}
+
+
+@dataclass(frozen=True)
+class Candidate:
+    order: Optional[str] = None
+    partition: int = 0
+    exec: str = "hier"
+    block: int = 256
+    direct: bool = False  # hierarchical: gather read rows from HBM/L2 (no staging)
+
+    def label(self) -> str:
+        o = self.order or "as-is"
+        p = f"+part{self.partition}" if self.partition else ""
+        d = "d" if self.direct and self.exec != "atomic" else ""
+        return f"{o}{p}/{self.exec}{d}/{self.block}"
+
+
+def default_candidates(loop: int, quick: bool = False) -> List[Candidate]:
+    orders = ["gps", "rcm"] if quick else [None, "random", "rcm", "gps"]
+    blocks = [128, 256] if quick else [128, 256, 512]
+    out = []
+    for o in orders:
+        out.append(Candidate(o, 0, "atomic", 256))
+        for b in blocks:
+            out.append(Candidate(o, 0, "hier", b))
+    if not quick:
+        for b in blocks:
+            out.append(Candidate("gps", b, "hier", b))
+            out.append(Candidate("rcm", b, "hier", b))
+    return out
+
+
+class OrderedCache:
+    """Host copies of a mesh after each ordering / partition, so that every
+    plan candidate starts from the same cell order."""
+
+    def __init__(self, md: mg.MeshData):
+        self.md = md
+        self._cache: Dict = {}
+
+    def get(self, order: Optional[str], partition: int) -> mg.MeshData:
+        key = (order, partition)
+        if key not in self._cache:
+            p = F.Problem.from_mesh(self.md)
+            t0 = time.perf_counter()
+            if order is not None:
+                p.reorder(ORDERS[order], seed=1)
+            if partition:
+                p.partition(partition)
+                p.reorder_to_partition()
+                p.renumber_points()
+            t_order = time.perf_counter() - t0
+            md2 = p.mesh_data()
+            md2.meta = dict(self.md.meta, order=order, partition=partition, order_s=t_order)
+            if partition:
+                md2.meta["partition_vector"] = p.partition_vector()
+            self._cache[key] = md2
+        return self._cache[key]
+
+
+def build(md: mg.MeshData, cand: Candidate, stream=None):
+    """A problem holding md (already ordered) and the candidate's plan."""
+    p = F.Problem.from_mesh(md)
+    flags = 0
+    if cand.partition:
+        p.set_partition(md.meta["partition_vector"])
+        flags |= F.PLAN_USE_PARTITION
+    if cand.direct:
+        flags |= F.PLAN_DIRECT_READS
+    plan = p.plan(EXECS[cand.exec], cand.block, flags)
+    return p, plan
+
+
+def time_plan(p, plan, iters: int = 10, warmup: int = 3, stream=None) -> float:
+    """Seconds per iteration (CUDA events on the launching stream)."""
+    import torch
+    st = stream or torch.cuda.current_stream()
+    plan.run(warmup, st)
+    p.sync(st)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record(st)
+    plan.run(iters, st)
+    end.record(st)
+    end.synchronize()
+    p.sync(st)
+    return start.elapsed_time(end) / 1e3 / iters
+
+
+def measure(cache: OrderedCache, cand: Candidate, iters: int = 10, warmup: int = 3) -> dict:
+    md = cache.get(cand.order, cand.partition)
+    try:
+        t0 = time.perf_counter()
+        p, plan = build(md, cand)
+        t_plan = time.perf_counter() - t0
+        secs = time_plan(p, plan, iters, warmup)
+        st = plan.stats()
+        ok = True
+    except F.FotError as e:
+        return {"cand": cand, "ok": False, "error": str(e)}
+    ub = cache.md.unique_bytes()
+    return {"cand": cand, "ok": ok, "seconds": secs, "gbs": ub / secs / 1e9,
+            "plan_s": t_plan, "order_s": md.meta.get("order_s", 0.0), "stats": st}
+
+
+def sweep(md: mg.MeshData, cands: List[Candidate], iters: int = 10, warmup: int = 3,
+          verbose: bool = False) -> List[dict]:
+    cache = OrderedCache(md)
+    out = []
+    for c in cands:
+        r = measure(cache, c, iters, warmup)
+        out.append(r)
+        if verbose:
+            if r["ok"]:
+                print(f"  {c.label():28s} {r['seconds']*1e6:9.1f} us  {r['gbs']:8.1f} GB/s", flush=True)
+            else:
+                print(f"  {c.label():28s} failed: {r['error']}", flush=True)
+    return out
+
+
+def best(results: List[dict]) -> dict:
+    ok = [r for r in results if r["ok"]]
+    return min(ok, key=lambda r: r["seconds"])

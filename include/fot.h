@@ -74,6 +74,8 @@ extern "C" {
 /* plan flags */
 #define FOT_PLAN_NO_AGGREGATE 1u /* atomic executor: no warp aggregation */
 #define FOT_PLAN_USE_PARTITION 2u /* hierarchical: blocks from the partition */
+#define FOT_PLAN_DIRECT_READS 4u  /* hierarchical: gather read rows from HBM/L2 instead of
+                                     staging them in shared memory */
 
 typedef struct fot_problem fot_problem;
 typedef struct fot_plan fot_plan;
@@ -238,6 +240,33 @@ int fot_batch_create(fot_problem *const *problems, fot_plan *const *plans,
 int fot_batch_run(fot_batch *b, uint32_t iterations, void *stream);
 int fot_batch_sync(fot_batch *b, void *stream);
 int fot_batch_destroy(fot_batch *b);
+
+/* ---- the learned plan cost model ------------------------------------------- */
+
+/* A 24 -> 64 -> 64 -> 1 ReLU MLP (FP32) predicting log(seconds per
+ * iteration) of a candidate plan from its feature vector; trained with the
+ * engine's own forward / backward / Adam kernels on timings the autotuner
+ * measured.  No counterpart in the reference. */
+#define FOT_MODEL_FEATURES 24
+#define FOT_MODEL_HIDDEN 64
+
+typedef struct fot_model fot_model;
+
+int fot_model_create(uint64_t seed, fot_model **out);
+int fot_model_destroy(fot_model *m);
+int fot_model_num_params(void);
+int fot_model_set_params(fot_model *m, const float *params);
+int fot_model_get_params(const fot_model *m, float *params);
+/* per-feature mean and standard deviation used to standardise inputs */
+int fot_model_set_normalisation(fot_model *m, const float *mean, const float *stddev);
+/* y[i] = model(X[i]) for n feature rows X (n x FOT_MODEL_FEATURES) */
+int fot_model_predict(fot_model *m, const float *X, int n, float *y);
+/* gradient of 0.5/n * sum (model(X) - t)^2 w.r.t. the parameters, and the loss */
+int fot_model_grad(fot_model *m, const float *X, const float *t, int n, float *grad, float *loss);
+/* `epochs` passes of Adam over contiguous minibatches of `batch` rows;
+ * epoch_loss (optional) receives the full-set loss after each epoch */
+int fot_model_train(fot_model *m, const float *X, const float *t, int n, int epochs, int batch,
+                    float lr, float weight_decay, float *epoch_loss);
 
 #ifdef __cplusplus
 }
