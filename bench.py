@@ -246,7 +246,8 @@ def main(argv=None):
         for c in T.default_candidates(md.loop, quick=True):
             sweep_res.append(T.measure(cache, c, iters=5, warmup=3))
         chosen = T.best(sweep_res)["cand"]
-    atomic_plain = T.measure(cache, T.Candidate(None, 0, "atomic", 256), iters=10, warmup=3)
+    atomic_plain = T.measure(cache, T.Candidate(None, 0, "atomic", 256, aggregate=False),
+                             iters=10, warmup=3)
 
     md_run = cache.get(chosen.order, chosen.partition)
     p, plan = T.build(md_run, chosen)
@@ -329,7 +330,8 @@ def main(argv=None):
                        "plan": chosen.label(), "plan_choice": choice_src,
                        "n_blocks": st["n_blocks"], "block_colours": st["n_colours"],
                        "parallelism": f"replicas x{world}"},
-            "atomic_baseline": {"plan": "as-is/atomic/256 (plain atomics on the random numbering)",
+            "atomic_baseline": {"plan": "as-is/atomic-plain/256 (one thread per face, f64 "
+                                        "atomics, no aggregation, on the given random numbering)",
                                 "value": atomic_plain.get("gbs"), "unit": "GB/s"},
             "speedup_vs_atomic": (value / world) / atomic_plain["gbs"] if atomic_plain.get("ok") else None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

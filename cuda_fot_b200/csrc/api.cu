@@ -145,9 +145,15 @@ fot::HierPlanDev fot_plan::dev(uint32_t iterations) const {
   }
   P.n_blocks = n_blocks;
   P.total_tiles = iterations * n_blocks;
-  for (int r = 0; r < 4; ++r) P.read_off[r] = read_off[r];
-  P.acc_off = acc_off;
-  P.pts_smem_off = pts_smem_off;
+  for (int r = 0; r < 4; ++r) P.read_off[r] = layout.read_off[r];
+  P.acc_off = layout.acc_off;
+  P.pts_smem_off = layout.pts_off;
+  P.rec = rec.as<unsigned char>();
+  P.rec_off = rec_off.as<uint32_t>();
+  P.buf_bytes = layout.buf_bytes;
+  P.inc_off = layout.inc_off;
+  P.outbuf_off = layout.outbuf_off;
+  P.block_done = block_done.as<unsigned int>();
   P.ctl = ctl.as<Ctl>();
   return P;
 }
@@ -362,12 +368,24 @@ int fot_plan_build(fot_problem *p, const fot_plan_desc *desc, fot_plan **out) {
     plan->threads = 256;
     rc = ops->occupancy(FOT_EXEC_ATOMIC, p->layout == FOT_SOA, 256, 0, 0, &plan->per_sm);
   } else if (desc->exec == FOT_EXEC_HIER || desc->exec == FOT_EXEC_HIER_LAUNCH) {
-    plan->variant = (desc->flags & FOT_PLAN_DIRECT_READS) ? 0u : 1u;
+    // staged reads by default; the persistent executor uses the pipelined
+    // kernel unless direct gathers or the simple tile loop are asked for
+    plan->variant = (desc->flags & FOT_PLAN_DIRECT_READS) ? 0u : kVariantStage;
+    if (desc->exec == FOT_EXEC_HIER && !(desc->flags & (FOT_PLAN_DIRECT_READS | FOT_PLAN_SIMPLE_TILES)))
+      plan->variant |= kVariantPipe;
     rc = build_hier_plan(p, plan);
     if (rc == FOT_OK) {
       plan->threads = hier_threads(desc->block_size);
-      plan->smem = ops->smem_layout(plan->cap[0], plan->cap[1], plan->variant, plan->read_off,
-                                    &plan->pts_smem_off, &plan->acc_off);
+      ops->smem_layout(plan->cap[0], plan->cap[1], plan->variant, plan->rec_cap, plan->threads,
+                       &plan->layout);
+      // the pipelined kernel holds two tiles' rows; when they do not fit,
+      // the single-buffer persistent kernel runs the plan instead
+      if ((plan->variant & kVariantPipe) && plan->layout.total > 227 * 1024) {
+        plan->variant &= ~kVariantPipe;
+        ops->smem_layout(plan->cap[0], plan->cap[1], plan->variant, plan->rec_cap,
+                         plan->threads, &plan->layout);
+      }
+      plan->smem = plan->layout.total;
       if (plan->smem > 227 * 1024)
         rc = fail(FOT_ERR_LIMIT,
                   "a block needs %zu bytes of shared memory (limit 227 KB): use a smaller block "
@@ -412,10 +430,22 @@ int fot_plan_build(fot_problem *p, const fot_plan_desc *desc, fot_plan **out) {
 }
 
 int fot_plan_destroy(fot_plan *plan) {
-  if (plan && plan->prob && plan->ctl.ptr && plan->prob->last_ctl == plan->ctl.as<Ctl>())
+  if (plan && plan->prob && plan->ctl.ptr && plan->prob->last_ctl == plan->ctl.as<Ctl>()) {
     plan->prob->last_ctl = nullptr;
+    plan->prob->last_flags = nullptr;
+    plan->prob->last_n_blocks = 0;
+  }
   delete plan;
   return FOT_OK;
+}
+
+// Remember the control block and flags of the last persistent run so that
+// fot_sync can report (and clear) device-side errors.
+static void note_run(fot_problem *p, fot_plan *plan) {
+  if (!plan->ctl.ptr) return;
+  p->last_ctl = plan->ctl.as<Ctl>();
+  p->last_flags = plan->block_done.ptr ? plan->block_done.as<unsigned int>() : nullptr;
+  p->last_n_blocks = plan->n_blocks;
 }
 
 int fot_plan_get_stats(const fot_plan *plan, fot_plan_stats *stats) {
@@ -489,7 +519,7 @@ static int run_plan(fot_problem *p, fot_plan *plan, uint32_t iterations, cudaStr
 
 int fot_run(fot_problem *p, fot_plan *plan, uint32_t iterations, void *stream) {
   FOT_TRY(run_plan(p, plan, iterations, static_cast<cudaStream_t>(stream)));
-  if (plan->ctl.ptr) p->last_ctl = plan->ctl.as<Ctl>();
+  note_run(p, plan);
   return FOT_OK;
 }
 
@@ -500,7 +530,9 @@ int fot_sync(fot_problem *p, void *stream) {
     Ctl c{};
     FOT_CUDA(cudaMemcpy(&c, p->last_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
     if (c.error) {
-      FOT_CUDA(cudaMemset(&p->last_ctl->error, 0, sizeof(unsigned int)));
+      // the run stopped early: restart the plan's queue and flags from zero
+      FOT_CUDA(cudaMemset(p->last_ctl, 0, sizeof(Ctl)));
+      if (p->last_flags) FOT_CUDA(cudaMemset(p->last_flags, 0, (size_t)p->last_n_blocks * 4));
       return fail(FOT_ERR_DEVICE, "a dependency wait of the persistent executor hit its limit");
     }
   }
@@ -531,6 +563,7 @@ int fot_graph_create(fot_problem *p, fot_plan *plan, uint32_t iterations, void *
   auto *g = new fot_graph();
   g->graph = graph;
   g->prob = p;
+  g->plan = plan;
   g->ctl = plan->ctl.as<Ctl>();
   const cudaError_t e2 = cudaGraphInstantiate(&g->exec, graph, 0);
   if (e2 != cudaSuccess) {
@@ -544,7 +577,7 @@ int fot_graph_create(fot_problem *p, fot_plan *plan, uint32_t iterations, void *
 int fot_graph_launch(fot_graph *g, void *stream) {
   if (!g) return fail(FOT_ERR_ARG, "null graph");
   FOT_CUDA(cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream)));
-  if (g->ctl) g->prob->last_ctl = g->ctl;
+  if (g->plan) note_run(g->prob, g->plan);
   return FOT_OK;
 }
 

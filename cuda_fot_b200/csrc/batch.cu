@@ -149,8 +149,14 @@ int fot_batch_create(fot_problem *const *problems, fot_plan *const *plans, uint3
     meshes[i].d = p->loop_data();
     meshes[i].P = pl->dev(1);
     meshes[i].loop = p->loop;
+    // the batched tiles use the staged one-tile-at-a-time layout
+    SmemLayout lay;
+    loop_ops(p->loop)->smem_layout(pl->cap[0], pl->cap[1], kVariantStage, 0, pl->threads, &lay);
+    for (int r = 0; r < 4; ++r) meshes[i].P.read_off[r] = lay.read_off[r];
+    meshes[i].P.acc_off = lay.acc_off;
+    meshes[i].P.pts_smem_off = lay.pts_off;
     B->threads = std::max(B->threads, pl->threads);
-    B->smem = std::max(B->smem, pl->smem);
+    B->smem = std::max(B->smem, lay.total);
     B->probs.push_back(p);
     B->plans.push_back(pl);
     B->versions.push_back(p->version);

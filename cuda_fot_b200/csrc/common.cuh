@@ -82,13 +82,21 @@ struct DevBuf {
 // write-back finished; exited: CTAs that left the claim loop (the last one
 // resets the three counters so the next launch starts from zero); error:
 // bit 0 = a dependency wait hit its limit.
+// base: iterations completed by all earlier launches (the per-block
+// completion flags of the pipelined executor count from it); the last CTA
+// advances it.
 struct Ctl {
   unsigned int ticket;
   unsigned int done;
   unsigned int exited;
   unsigned int error;
-  unsigned int pad[4];
+  unsigned int base;
+  unsigned int pad[3];
 };
+
+__device__ __forceinline__ void st_release_gpu(unsigned int *p, unsigned int v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 constexpr unsigned int kErrWaitLimit = 1u;
 // Upper bound of the dependency-wait polls (each followed by a ~256 ns
@@ -121,6 +129,56 @@ __device__ __forceinline__ void cp_async4(void *dst, const void *src) {
 }
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N> __device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// mbarrier + 1D bulk copy (TMA engine, no tensor map, no multicast) of a
+// 16-byte aligned segment of this GPU's global memory into shared memory.
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned phase) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_timer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait for an mbarrier phase: gives up (returns false) after about
+// two seconds of wall time.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned phase) {
+  if (mbar_try_wait(bar, phase)) return true;
+  const uint64_t t0 = global_timer_ns();
+  for (unsigned i = 1;; ++i) {
+    if (mbar_try_wait(bar, phase)) return true;
+    if ((i & 63u) == 0 && global_timer_ns() - t0 > 2000000000ull) return false;
+  }
 }
 
 } // namespace fot

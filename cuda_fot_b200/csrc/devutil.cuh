@@ -12,15 +12,31 @@ namespace fot {
 
 inline uint32_t blocks_for(size_t n, uint32_t t = 256) { return (uint32_t)((n + t - 1) / t); }
 
+// Grow-only temporary storage of the CUB calls below (one per host thread,
+// per device), so that the many small sorts of the level-by-level orderings
+// do not allocate and free device memory every time.
+inline int cub_scratch(size_t bytes, void **ptr) {
+  struct Scratch {
+    DevBuf buf[16];
+  };
+  static thread_local Scratch s;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  DevBuf &b = s.buf[dev & 15];
+  if (b.bytes < bytes) FOT_TRY(b.alloc(bytes + bytes / 2 + 4096));
+  *ptr = b.ptr;
+  return FOT_OK;
+}
+
 template <class K, class V>
 int sort_pairs(const K *kin, K *kout, const V *vin, V *vout, size_t n, cudaStream_t st = 0,
                int end_bit = sizeof(K) * 8) {
   if (n == 0) return FOT_OK;
   size_t tb = 0;
   FOT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, vin, vout, (int)n, 0, end_bit, st));
-  DevBuf tmp;
-  FOT_TRY(tmp.alloc(tb));
-  FOT_CUDA(cub::DeviceRadixSort::SortPairs(tmp.ptr, tb, kin, kout, vin, vout, (int)n, 0, end_bit, st));
+  void *tmp = nullptr;
+  FOT_TRY(cub_scratch(tb, &tmp));
+  FOT_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, kin, kout, vin, vout, (int)n, 0, end_bit, st));
   return FOT_OK;
 }
 
@@ -28,9 +44,9 @@ template <class K> int sort_keys(const K *kin, K *kout, size_t n, cudaStream_t s
   if (n == 0) return FOT_OK;
   size_t tb = 0;
   FOT_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tb, kin, kout, (int)n, 0, sizeof(K) * 8, st));
-  DevBuf tmp;
-  FOT_TRY(tmp.alloc(tb));
-  FOT_CUDA(cub::DeviceRadixSort::SortKeys(tmp.ptr, tb, kin, kout, (int)n, 0, sizeof(K) * 8, st));
+  void *tmp = nullptr;
+  FOT_TRY(cub_scratch(tb, &tmp));
+  FOT_CUDA(cub::DeviceRadixSort::SortKeys(tmp, tb, kin, kout, (int)n, 0, sizeof(K) * 8, st));
   return FOT_OK;
 }
 
@@ -42,9 +58,9 @@ template <class K> int unique_keys(const K *in, K *out, size_t n, uint32_t *coun
   FOT_TRY(nsel.alloc(4));
   size_t tb = 0;
   FOT_CUDA(cub::DeviceSelect::Unique(nullptr, tb, in, out, nsel.as<uint32_t>(), (int)n, st));
-  DevBuf tmp;
-  FOT_TRY(tmp.alloc(tb));
-  FOT_CUDA(cub::DeviceSelect::Unique(tmp.ptr, tb, in, out, nsel.as<uint32_t>(), (int)n, st));
+  void *tmp = nullptr;
+  FOT_TRY(cub_scratch(tb, &tmp));
+  FOT_CUDA(cub::DeviceSelect::Unique(tmp, tb, in, out, nsel.as<uint32_t>(), (int)n, st));
   FOT_CUDA(cudaMemcpyAsync(count, nsel.ptr, 4, cudaMemcpyDeviceToHost, st));
   FOT_CUDA(cudaStreamSynchronize(st));
   return FOT_OK;
@@ -54,9 +70,9 @@ template <class T> int excl_sum(const T *in, T *out, size_t n, cudaStream_t st =
   if (n == 0) return FOT_OK;
   size_t tb = 0;
   FOT_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, (int)n, st));
-  DevBuf tmp;
-  FOT_TRY(tmp.alloc(tb));
-  FOT_CUDA(cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, in, out, (int)n, st));
+  void *tmp = nullptr;
+  FOT_TRY(cub_scratch(tb, &tmp));
+  FOT_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, in, out, (int)n, st));
   return FOT_OK;
 }
 

@@ -12,9 +12,24 @@
 
 namespace fot {
 
+// Shared-memory layout of a hierarchical tile kernel.
+struct SmemLayout {
+  uint32_t read_off[4] = {0, 0, 0, 0}; // read set rows (relative to a pipeline buffer)
+  uint32_t pts_off = 0;                // point lists (non-pipelined kernels)
+  uint32_t acc_off = 0;                // accumulator (non-pipelined kernels)
+  uint32_t buf_bytes = 0;              // one pipeline buffer: tile record + read rows
+  uint32_t inc_off = 0;                // per-slot increments (pipelined kernel)
+  uint32_t outbuf_off = 0;             // prefetched output rows (pipelined kernel)
+  size_t total = 0;                    // bytes per CTA
+};
+
 // Per-loop entry points, one table per loop translation unit (loop_*.cu).
 // `variant` selects the hierarchical tile kernel: bit 0 = stage the read rows
-// in shared memory (else gather them straight from HBM/L2).
+// in shared memory (else gather them straight from HBM/L2); bit 1 = the
+// pipelined persistent kernel (tile records by bulk copy, double-buffered
+// staging, per-point gather of the increments).
+constexpr uint32_t kVariantStage = 1u, kVariantPipe = 2u;
+
 struct LoopOps {
   // launch one iteration of the atomic executor
   int (*run_atomic)(const LoopData &d, bool soa, bool aggregate, uint32_t threads,
@@ -30,10 +45,9 @@ struct LoopOps {
   int (*occupancy)(int exec, bool soa, uint32_t threads, uint32_t variant, size_t smem,
                    int *per_sm);
   // shared-memory layout of a hierarchical tile for at most cap0 / cap1
-  // points per block: byte offsets of the read sets, the point lists and the
-  // accumulator; returns the bytes per CTA
-  size_t (*smem_layout)(uint32_t cap0, uint32_t cap1, uint32_t variant, uint32_t read_off[4],
-                        uint32_t *pts_off, uint32_t *acc_off);
+  // points per block and tile records of at most rec_cap bytes
+  void (*smem_layout)(uint32_t cap0, uint32_t cap1, uint32_t variant, uint32_t rec_cap,
+                      uint32_t threads, SmemLayout *out);
 };
 
 const LoopOps *loop_ops(int loop);
@@ -71,6 +85,8 @@ struct fot_problem {
   uint64_t version = 1; // bumped whenever cells or points are renumbered
   int device = 0;
   fot::Ctl *last_ctl = nullptr; // control block of the last persistent run
+  unsigned int *last_flags = nullptr; // its per-block completion flags
+  uint32_t last_n_blocks = 0;
 
   size_t point_bytes(uint32_t k) const {
     return (size_t)n_points[k] * info.point_dim[k] * info.point_type_size[k];
@@ -95,10 +111,11 @@ struct fot_plan {
   fot::DevBuf block_start, block_wait, block_ntcol, tcol;
   fot::DevBuf pts_off[2], pts[2], lidx[2];
   fot::DevBuf build_perm; // position -> cell index before the build
+  fot::DevBuf rec, rec_off; // tile records (see plan.cu)
+  fot::DevBuf block_done;   // per block: completed iterations (pipelined executor)
+  uint32_t rec_cap = 0;
   uint32_t cap[2] = {0, 0};
-  uint32_t read_off[4] = {0, 0, 0, 0};
-  uint32_t acc_off = 0;
-  uint32_t pts_smem_off = 0;
+  fot::SmemLayout layout;
   size_t smem = 0;
   uint32_t threads = 0;
   int per_sm = 0;
@@ -110,6 +127,7 @@ struct fot_graph {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   fot_problem *prob = nullptr;
+  fot_plan *plan = nullptr;
   fot::Ctl *ctl = nullptr;
   ~fot_graph() {
     if (exec) cudaGraphExecDestroy(exec);

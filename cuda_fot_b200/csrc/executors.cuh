@@ -57,6 +57,13 @@ struct HierPlanDev {
   uint32_t acc_off;            // shared-memory byte offset of the accumulator
   uint32_t pts_smem_off;       // shared-memory byte offset of the tile's point lists
   Ctl *ctl;
+  // pipelined kernel
+  const unsigned char *rec;    // tile records
+  const uint32_t *rec_off;     // n_blocks+1 byte offsets of the records
+  uint32_t buf_bytes;          // one pipeline buffer (record region + read rows)
+  uint32_t inc_off;            // per-slot increments
+  uint32_t outbuf_off;         // prefetched output rows
+  unsigned int *block_done;    // per block: completed iterations (relative to ctl->base)
 };
 
 // Direct (cell) data of one cell: SOA with stride n_cells.
@@ -210,3 +217,4 @@ __global__ void __launch_bounds__(256, (65536 / (256 * L::kRegCap)) > 0 ? 65536 
 } // namespace fot
 
 #include "hier.cuh"
+#include "hier_pipe.cuh"

@@ -41,11 +41,23 @@ template <bool SOA, bool STAGE> const void *hier_kernel_t(bool persistent, uint3
   return nullptr;
 }
 
-// variant bit 0: staged reads
+template <bool SOA> const void *pipe_kernel(uint32_t threads) {
+  switch (threads) {
+  case 128: return reinterpret_cast<const void *>(&k_hier_pipe<L, SOA, 128>);
+  case 256: return reinterpret_cast<const void *>(&k_hier_pipe<L, SOA, 256>);
+  case 512: return reinterpret_cast<const void *>(&k_hier_pipe<L, SOA, 512>);
+  case 1024: return reinterpret_cast<const void *>(&k_hier_pipe<L, SOA, 1024>);
+  }
+  return nullptr;
+}
+
+// variant: kVariantStage (staged reads), kVariantPipe (pipelined kernel)
 const void *kernel_for(int exec, bool soa, uint32_t threads, uint32_t variant) {
   if (exec == FOT_EXEC_ATOMIC)
     return soa ? reinterpret_cast<const void *>(&k_atomic<L, true, true>)
                : reinterpret_cast<const void *>(&k_atomic<L, false, true>);
+  if (exec == FOT_EXEC_HIER && (variant & kVariantPipe))
+    return soa ? pipe_kernel<true>(threads) : pipe_kernel<false>(threads);
   const bool persistent = exec == FOT_EXEC_HIER;
   const bool stage = variant & 1u;
   if (soa) return stage ? hier_kernel_t<true, true>(persistent, threads)
@@ -89,25 +101,46 @@ int occupancy(int exec, bool soa, uint32_t threads, uint32_t variant, size_t sme
   return FOT_OK;
 }
 
-size_t smem_layout(uint32_t cap0, uint32_t cap1, uint32_t variant, uint32_t read_off[4],
-                   uint32_t *pts_off, uint32_t *acc_off) {
-  const bool stage = variant & 1u;
+void smem_layout(uint32_t cap0, uint32_t cap1, uint32_t variant, uint32_t rec_cap,
+                 uint32_t threads, SmemLayout *out) {
+  using out_t = typename L::out_t;
+  using read_t = typename L::read_t;
+  const bool stage = variant & kVariantStage;
+  auto a16 = [](size_t v) { return (v + 15) & ~size_t(15); };
+  SmemLayout s;
   size_t off = 0;
-  for (int r = 0; r < 4; ++r) read_off[r] = 0;
+  if (variant & kVariantPipe) {
+    // buffer = [tile record][read rows]; two buffers, then the increments and
+    // the prefetched output rows
+    off = a16(rec_cap);
+    for (int r = 0; r < L::kNumRead; ++r) {
+      s.read_off[r] = (uint32_t)off;
+      const uint32_t cap = L::read_class(r) == 0 ? cap0 : cap1;
+      off = a16(off + (size_t)cap * L::read_dim(r) * sizeof(read_t));
+    }
+    s.buf_bytes = (uint32_t)((off + 127) & ~size_t(127));
+    off = 2 * (size_t)s.buf_bytes;
+    s.inc_off = (uint32_t)off;
+    off = a16(off + (size_t)L::kOut * L::kDim * threads * sizeof(out_t));
+    s.outbuf_off = (uint32_t)off;
+    if ((L::kOut * sizeof(out_t)) % 16 == 0) off = a16(off + (size_t)cap0 * L::kOut * sizeof(out_t));
+    s.total = off;
+    *out = s;
+    return;
+  }
   if (stage) {
     for (int r = 0; r < L::kNumRead; ++r) {
-      read_off[r] = (uint32_t)off;
+      s.read_off[r] = (uint32_t)off;
       const uint32_t cap = L::read_class(r) == 0 ? cap0 : cap1;
-      off += (size_t)cap * L::read_dim(r) * sizeof(typename L::read_t);
-      off = (off + 15) & ~size_t(15);
+      off = a16(off + (size_t)cap * L::read_dim(r) * sizeof(read_t));
     }
   }
-  *acc_off = (uint32_t)off;
-  off += (size_t)cap0 * L::kOut * sizeof(typename L::out_t);
-  off = (off + 15) & ~size_t(15);
-  *pts_off = (uint32_t)off;
+  s.acc_off = (uint32_t)off;
+  off = a16(off + (size_t)cap0 * L::kOut * sizeof(out_t));
+  s.pts_off = (uint32_t)off;
   off += (size_t)(cap0 + (stage && L::kHasClass1 ? cap1 : 0)) * sizeof(uint32_t);
-  return (off + 15) & ~size_t(15);
+  s.total = a16(off);
+  *out = s;
 }
 
 } // namespace FOT_ADAPTER_NS

@@ -280,6 +280,103 @@ __global__ void k_gather_plan(GatherArgs g) {
 }
 
 // ---------------------------------------------------------------------------
+// step 4b: tile records -- everything a tile needs besides the read rows, in
+// one 16-byte aligned segment per block so one bulk copy brings it in:
+//   u32 header[8] = {start, ncell, n0, n1, ntcol, wait, ndep, block}
+//   u32 pts0[n0], u32 pts1[n1], u16 lidx0[D][ncell], u16 lidx1[D][ncell],
+//   u16 pc_off[n0 + 1], u16 pc_idx[D * ncell], (pad to 4 bytes),
+//   u32 dep[ndep], zero padding to 16 bytes
+// pc_off / pc_idx list, for each written point j of the block, its
+// contributions e = s * T + i (slot s of the block's i-th cell; T = threads
+// per CTA) in increasing (i, s) order -- cells are sorted by thread colour, so
+// this is the thread-colour order of the reference's shared-memory
+// accumulation (res_calc.hpp:328-339).
+// dep lists the blocks sharing a written point with this one (the conflict
+// graph); bit 31 marks those of an earlier block colour.
+// ---------------------------------------------------------------------------
+struct RecordArgs {
+  const uint32_t *block_start, *block_wait, *pts_off[2], *pts[2], *rec_off;
+  const uint16_t *lidx[2];
+  const uint8_t *ntcol;
+  const uint32_t *dep_off, *dep;
+  unsigned char *rec;
+  uint32_t n_cells, threads;
+  int n_class, D;
+};
+
+__host__ __device__ inline uint32_t record_dep_offset(uint32_t ncell, uint32_t n0, uint32_t n1,
+                                                      int D, int n_class) {
+  const uint32_t b = 32 + 4 * (n0 + n1) + 2 * D * ncell * n_class + 2 * (n0 + 1) + 2 * D * ncell;
+  return (b + 3) & ~3u;
+}
+
+__host__ __device__ inline uint32_t record_bytes(uint32_t ncell, uint32_t n0, uint32_t n1, int D,
+                                                 int n_class, uint32_t ndep) {
+  return (record_dep_offset(ncell, n0, n1, D, n_class) + 4 * ndep + 15) & ~15u;
+}
+
+__global__ void k_build_records(RecordArgs a) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t start = a.block_start[b], ncell = a.block_start[b + 1] - start;
+  uint32_t n[2] = {a.pts_off[0][b + 1] - a.pts_off[0][b], 0};
+  if (a.n_class > 1) n[1] = a.pts_off[1][b + 1] - a.pts_off[1][b];
+  unsigned char *r = a.rec + a.rec_off[b];
+  uint32_t *h = reinterpret_cast<uint32_t *>(r);
+  if (threadIdx.x == 0) {
+    h[0] = start;
+    h[1] = ncell;
+    h[2] = n[0];
+    h[3] = n[1];
+    h[4] = a.ntcol[b];
+    h[5] = a.block_wait[b];
+    h[6] = a.dep_off[b + 1] - a.dep_off[b];
+    h[7] = b;
+  }
+  uint32_t *pts = h + 8;
+  for (int c = 0; c < a.n_class; ++c) {
+    for (uint32_t i = threadIdx.x; i < n[c]; i += blockDim.x) pts[i] = a.pts[c][a.pts_off[c][b] + i];
+    pts += n[c];
+  }
+  uint16_t *l = reinterpret_cast<uint16_t *>(pts);
+  for (int c = 0; c < a.n_class; ++c)
+    for (int s = 0; s < a.D; ++s) {
+      for (uint32_t i = threadIdx.x; i < ncell; i += blockDim.x)
+        l[i] = a.lidx[c][(size_t)s * a.n_cells + start + i];
+      l += ncell;
+    }
+  // contributions per written point: counts, offsets, then each thread
+  // collects the entries of its own points by scanning all of them in order
+  uint16_t *pc_off = l;
+  uint16_t *pc_idx = l + n[0] + 1;
+  const uint16_t *l0 = reinterpret_cast<const uint16_t *>(h + 8 + n[0] + n[1]);
+  const uint32_t E = a.D * ncell;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (uint32_t j = 0; j <= n[0]; ++j) pc_off[j] = 0;
+    for (uint32_t i = 0; i < ncell; ++i)
+      for (int s = 0; s < a.D; ++s) pc_off[l0[s * ncell + i] + 1]++;
+    for (uint32_t j = 0; j < n[0]; ++j) pc_off[j + 1] += pc_off[j];
+  }
+  __syncthreads();
+  for (uint32_t j0 = 0; j0 < n[0]; j0 += blockDim.x) {
+    const uint32_t j = j0 + threadIdx.x;
+    uint32_t w = j < n[0] ? pc_off[j] : 0;
+    for (uint32_t i = 0; i < ncell; ++i)
+      for (int s = 0; s < a.D; ++s)
+        if (j < n[0] && l0[s * ncell + i] == j) pc_idx[w++] = (uint16_t)(s * a.threads + i);
+  }
+  const uint32_t dep_at = record_dep_offset(ncell, n[0], n[1], a.D, a.n_class);
+  const uint32_t ndep = a.dep_off[b + 1] - a.dep_off[b];
+  for (uint32_t i = (uint32_t)(reinterpret_cast<unsigned char *>(pc_idx + E) - r) + threadIdx.x;
+       i < dep_at; i += blockDim.x)
+    r[i] = 0;
+  uint32_t *dep = reinterpret_cast<uint32_t *>(r + dep_at);
+  for (uint32_t i = threadIdx.x; i < ndep; i += blockDim.x) dep[i] = a.dep[a.dep_off[b] + i];
+  const uint32_t used = dep_at + 4 * ndep;
+  for (uint32_t i = used + threadIdx.x; i < a.rec_off[b + 1] - a.rec_off[b]; i += blockDim.x) r[i] = 0;
+}
+
+// ---------------------------------------------------------------------------
 // step 5: permute the problem's cells (rows of the mappings, cell datasets)
 // ---------------------------------------------------------------------------
 __global__ void k_gather_rows_u32(const uint32_t *src, uint32_t *dst, const uint32_t *perm,
@@ -310,7 +407,8 @@ template <int ITEMS> int launch_local(const LocalOut &o, uint32_t nfb, size_t dy
 
 // Colour the blocks; returns per-formation-block colours on the host.
 static int colour_blocks(const DevBuf &pad0, const DevBuf &cnt0, uint32_t nfb, uint32_t cap,
-                         std::vector<int> &colours, DevBuf &d_err) {
+                         std::vector<int> &colours, DevBuf &d_err, std::vector<uint32_t> &g_row,
+                         std::vector<uint32_t> &g_col) {
   std::vector<uint32_t> h_cnt;
   FOT_TRY(download(h_cnt, cnt0, nfb));
   std::vector<uint32_t> h_off(nfb);
@@ -391,6 +489,13 @@ static int colour_blocks(const DevBuf &pad0, const DevBuf &cnt0, uint32_t nfb, u
     FOT_CUDA(cudaGetLastError());
     FOT_CUDA(cudaMemcpy(&n_done, done.ptr, 4, cudaMemcpyDeviceToHost));
   }
+  // the conflict graph (CSR over formation blocks) for the per-block
+  // dependencies of the pipelined executor
+  FOT_TRY(download(g_row, row, nfb + 1));
+  std::vector<uint64_t> edges;
+  FOT_TRY(download(edges, e0.as<uint64_t>(), n_unique));
+  g_col.resize(n_unique);
+  for (uint32_t e = 0; e < n_unique; ++e) g_col[e] = (uint32_t)edges[e];
   return download(colours, col, nfb);
 }
 
@@ -472,7 +577,8 @@ int build_hier_plan(fot_problem *p, fot_plan *plan) {
 
   // 3. block colours
   std::vector<int> colours;
-  FOT_TRY(colour_blocks(pad[0], cnt[0], nfb, cap, colours, d_err));
+  std::vector<uint32_t> g_row, g_col;
+  FOT_TRY(colour_blocks(pad[0], cnt[0], nfb, cap, colours, d_err, g_row, g_col));
   int h_err = 0;
   FOT_CUDA(cudaMemcpy(&h_err, d_err.ptr, 4, cudaMemcpyDeviceToHost));
   if (h_err & 1) return fail(FOT_ERR_LIMIT, "a block needs more than %d thread colours", kMaxThreadColours);
@@ -542,6 +648,60 @@ int build_hier_plan(fot_problem *p, fot_plan *plan) {
   }
   k_gather_plan<<<nfb, 256>>>(g);
   FOT_CUDA(cudaGetLastError());
+
+  // 4b. tile records
+  {
+    // conflict neighbours of each block in final order; bit 31: earlier colour
+    std::vector<uint32_t> final_of(nfb);
+    for (uint32_t b = 0; b < nfb; ++b) final_of[order[b]] = b;
+    std::vector<uint32_t> dep_off(nfb + 1, 0), dep;
+    for (uint32_t b = 0; b < nfb; ++b) {
+      const uint32_t fb = order[b];
+      for (uint32_t e = g_row[fb]; e < g_row[fb + 1]; ++e) {
+        const uint32_t fn = g_col[e];
+        dep.push_back(final_of[fn] | (colours[fn] < colours[fb] ? 0x80000000u : 0u));
+      }
+      dep_off[b + 1] = (uint32_t)dep.size();
+    }
+    DevBuf d_dep_off, d_dep;
+    FOT_TRY(upload(d_dep_off, dep_off));
+    FOT_TRY(upload(d_dep, dep));
+    std::vector<uint32_t> rec_off(nfb + 1, 0);
+    uint32_t rec_cap = 0;
+    for (uint32_t b = 0; b < nfb; ++b) {
+      const uint32_t ncell = block_start[b + 1] - block_start[b];
+      const uint32_t n0 = h_off[0][b + 1] - h_off[0][b];
+      const uint32_t n1 = n_class > 1 ? h_off[1][b + 1] - h_off[1][b] : 0;
+      const uint32_t padded = record_bytes(ncell, n0, n1, D, n_class, dep_off[b + 1] - dep_off[b]);
+      rec_cap = std::max(rec_cap, padded);
+      rec_off[b + 1] = rec_off[b] + padded;
+    }
+    FOT_TRY(upload(plan->rec_off, rec_off));
+    FOT_TRY(plan->rec.alloc(rec_off[nfb]));
+    plan->rec_cap = rec_cap;
+    // completed iterations of each block (the dependency flags)
+    FOT_TRY(plan->block_done.alloc((size_t)nfb * 4));
+    FOT_CUDA(cudaMemset(plan->block_done.ptr, 0, (size_t)nfb * 4));
+    RecordArgs ra{};
+    ra.block_start = plan->block_start.as<uint32_t>();
+    ra.block_wait = plan->block_wait.as<uint32_t>();
+    ra.rec_off = plan->rec_off.as<uint32_t>();
+    ra.threads = hier_threads(B);
+    ra.dep_off = d_dep_off.as<uint32_t>();
+    ra.dep = d_dep.as<uint32_t>();
+    ra.ntcol = plan->block_ntcol.as<uint8_t>();
+    ra.rec = plan->rec.as<unsigned char>();
+    ra.n_cells = n;
+    ra.n_class = n_class;
+    ra.D = D;
+    for (int c = 0; c < n_class; ++c) {
+      ra.pts_off[c] = plan->pts_off[c].as<uint32_t>();
+      ra.pts[c] = plan->pts[c].as<uint32_t>();
+      ra.lidx[c] = plan->lidx[c].as<uint16_t>();
+    }
+    k_build_records<<<nfb, 128>>>(ra);
+    FOT_CUDA(cudaGetLastError());
+  }
 
   // 5. permute the problem's cells into plan order
   const uint32_t *perm = plan->build_perm.as<uint32_t>();

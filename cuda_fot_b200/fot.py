@@ -29,7 +29,7 @@ FOT_OK = 0
 AOS, SOA = 0, 1
 EXEC_ATOMIC, EXEC_HIER, EXEC_HIER_LAUNCH = 0, 1, 2
 ORDER_NATURAL, ORDER_RANDOM, ORDER_RCM, ORDER_GPS = 0, 1, 2, 3
-PLAN_NO_AGGREGATE, PLAN_USE_PARTITION, PLAN_DIRECT_READS = 1, 2, 4
+PLAN_NO_AGGREGATE, PLAN_USE_PARTITION, PLAN_DIRECT_READS, PLAN_SIMPLE_TILES = 1, 2, 4, 8
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(f"{LIB_PATH} is missing: build it with `python -m cuda_fot_b200.build`")

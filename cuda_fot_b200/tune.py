@@ -40,12 +40,14 @@ class Candidate:
     exec: str = "hier"
     block: int = 256
     direct: bool = False  # hierarchical: gather read rows from HBM/L2 (no staging)
+    aggregate: bool = True  # atomic: warp aggregation of same-target lanes
 
     def label(self) -> str:
         o = self.order or "as-is"
         p = f"+part{self.partition}" if self.partition else ""
         d = "d" if self.direct and self.exec != "atomic" else ""
-        return f"{o}{p}/{self.exec}{d}/{self.block}"
+        a = "-plain" if self.exec == "atomic" and not self.aggregate else ""
+        return f"{o}{p}/{self.exec}{d}{a}/{self.block}"
 
 
 def default_candidates(loop: int, quick: bool = False) -> List[Candidate]:
@@ -100,6 +102,8 @@ def build(md: mg.MeshData, cand: Candidate, stream=None):
         flags |= F.PLAN_USE_PARTITION
     if cand.direct:
         flags |= F.PLAN_DIRECT_READS
+    if cand.exec == "atomic" and not cand.aggregate:
+        flags |= F.PLAN_NO_AGGREGATE
     plan = p.plan(EXECS[cand.exec], cand.block, flags)
     return p, plan
 

@@ -76,6 +76,8 @@ extern "C" {
 #define FOT_PLAN_USE_PARTITION 2u /* hierarchical: blocks from the partition */
 #define FOT_PLAN_DIRECT_READS 4u  /* hierarchical: gather read rows from HBM/L2 instead of
                                      staging them in shared memory */
+#define FOT_PLAN_SIMPLE_TILES 8u  /* persistent hierarchical: one tile at a time with a
+                                     barrier per thread colour (no pipelining) */
 
 typedef struct fot_problem fot_problem;
 typedef struct fot_plan fot_plan;

@@ -60,14 +60,20 @@ def test_atomic_matches_serial(loop, layout, aggregate):
         assert bitwise_equal(p.cell_weights(j), ref)
 
 
+KERNELS = {  # executor, plan flags
+    "pipelined": (1, 0), "simple": (1, 8), "direct": (1, 4), "per_colour": (2, 0),
+}
+
+
 @pytest.mark.parametrize("layout", ["aos", "soa"])
 @pytest.mark.parametrize("loop", range(5))
 @pytest.mark.parametrize("block", [32, 128, 256])
-@pytest.mark.parametrize("persistent", [True, False])
-def test_hierarchical_bit_exact_replay(loop, layout, block, persistent):
+@pytest.mark.parametrize("kernel", list(KERNELS))
+def test_hierarchical_bit_exact_replay(loop, layout, block, kernel):
     md = medium(loop, layout)
     p = F().Problem.from_mesh(md)
-    plan = p.plan(F().EXEC_HIER if persistent else F().EXEC_HIER_LAUNCH, block)
+    exec_, flags = KERNELS[kernel]
+    plan = p.plan(exec_, block, flags)
     ex = plan.export()
     rc, msg = O.check_plan(ex, md.maps[0], md.n_points[0], block)
     assert rc == 0, msg
