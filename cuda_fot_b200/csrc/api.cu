@@ -150,9 +150,12 @@ fot::HierPlanDev fot_plan::dev(uint32_t iterations) const {
   P.pts_smem_off = layout.pts_off;
   P.rec = rec.as<unsigned char>();
   P.rec_off = rec_off.as<uint32_t>();
-  P.buf_bytes = layout.buf_bytes;
+  P.rec_slot = layout.rec_slot;
+  P.rows_off = layout.rows_off;
+  P.rows_bytes = layout.rows_bytes;
   P.inc_off = layout.inc_off;
   P.outbuf_off = layout.outbuf_off;
+  P.outbuf_bytes = layout.outbuf_bytes;
   P.block_done = block_done.as<unsigned int>();
   P.ctl = ctl.as<Ctl>();
   return P;
@@ -371,7 +374,10 @@ int fot_plan_build(fot_problem *p, const fot_plan_desc *desc, fot_plan **out) {
     // staged reads by default; the persistent executor uses the pipelined
     // kernel unless direct gathers or the simple tile loop are asked for
     plan->variant = (desc->flags & FOT_PLAN_DIRECT_READS) ? 0u : kVariantStage;
-    if (desc->exec == FOT_EXEC_HIER && !(desc->flags & (FOT_PLAN_DIRECT_READS | FOT_PLAN_SIMPLE_TILES)))
+    // (its two control warps need room beside the compute threads: blocks of
+    // at most 512 cells)
+    if (desc->exec == FOT_EXEC_HIER && desc->block_size <= 512 &&
+        !(desc->flags & (FOT_PLAN_DIRECT_READS | FOT_PLAN_SIMPLE_TILES)))
       plan->variant |= kVariantPipe;
     rc = build_hier_plan(p, plan);
     if (rc == FOT_OK) {

@@ -17,17 +17,19 @@ struct SmemLayout {
   uint32_t read_off[4] = {0, 0, 0, 0}; // read set rows (relative to a pipeline buffer)
   uint32_t pts_off = 0;                // point lists (non-pipelined kernels)
   uint32_t acc_off = 0;                // accumulator (non-pipelined kernels)
-  uint32_t buf_bytes = 0;              // one pipeline buffer: tile record + read rows
-  uint32_t inc_off = 0;                // per-slot increments (pipelined kernel)
-  uint32_t outbuf_off = 0;             // prefetched output rows (pipelined kernel)
+  // pipelined kernel: 4 record slots, 2 read-row slots, the increments,
+  // 2 output-row slots
+  uint32_t rec_slot = 0, rows_off = 0, rows_bytes = 0;
+  uint32_t inc_off = 0, outbuf_off = 0, outbuf_bytes = 0;
   size_t total = 0;                    // bytes per CTA
 };
 
 // Per-loop entry points, one table per loop translation unit (loop_*.cu).
 // `variant` selects the hierarchical tile kernel: bit 0 = stage the read rows
 // in shared memory (else gather them straight from HBM/L2); bit 1 = the
-// pipelined persistent kernel (tile records by bulk copy, double-buffered
-// staging, per-point gather of the increments).
+// pipelined persistent kernel (warp-specialised: tile records by bulk copy,
+// double-buffered staging, per-point gather of the increments), launched
+// with 64 threads more than `threads` for its two control warps.
 constexpr uint32_t kVariantStage = 1u, kVariantPipe = 2u;
 
 struct LoopOps {

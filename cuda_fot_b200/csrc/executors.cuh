@@ -60,9 +60,12 @@ struct HierPlanDev {
   // pipelined kernel
   const unsigned char *rec;    // tile records
   const uint32_t *rec_off;     // n_blocks+1 byte offsets of the records
-  uint32_t buf_bytes;          // one pipeline buffer (record region + read rows)
+  uint32_t rec_slot;           // bytes of one tile-record slot (slots start at offset 0)
+  uint32_t rows_off;           // first read-row slot (read_off[] are relative to a slot)
+  uint32_t rows_bytes;         // bytes of one read-row slot
   uint32_t inc_off;            // per-slot increments
-  uint32_t outbuf_off;         // prefetched output rows
+  uint32_t outbuf_off;         // first prefetched-output-row slot
+  uint32_t outbuf_bytes;       // bytes of one output-row slot
   unsigned int *block_done;    // per block: completed iterations (relative to ctl->base)
 };
 

@@ -1,22 +1,29 @@
-// The pipelined persistent hierarchical-colour kernel (variant kVariantPipe).
+// The pipelined persistent hierarchical-colour kernel (variant kVariantPipe),
+// warp-specialised.
 //
-// Each CTA runs a two-deep software pipeline over the tiles it claims (tiles
-// = blocks in block-colour order, iteration after iteration):
-//   * a tile's RECORD (header, point lists, local indices, per-point
-//     contribution lists; built by plan.cu) arrives by one bulk copy on the
-//     TMA engine, completing an mbarrier, one tile ahead;
-//   * the tile's READ ROWS are staged with cp.async into the same pipeline
-//     buffer while the previous tile computes and writes back;
-//   * if the tile's dependency (all tiles of the earlier block colours
-//     written back) already holds when the tile starts, its OUTPUT ROWS are
-//     prefetched too, so the write-back is a plain store;
-//   * compute: each thread computes its cell's per-slot increments into a
-//     shared buffer; one barrier; then each thread owns written points and
-//     sums their contributions in thread-colour order -- the order of the
-//     reference's colour-by-colour shared accumulation, so results stay
-//     bit-identical to the CPU replay -- and writes out[p] += sum.
-// Three CTA barriers per tile instead of one per thread colour; every wait is
-// bounded (mbarrier waits by wall time, the dependency wait by polls).
+// A CTA runs T compute threads and two control warps over the tiles it
+// claims (tiles = blocks in block-colour order, iteration after iteration):
+//   * the RECORD warp claims tiles from the plan's queue and copies each
+//     tile's record (header, point lists, local indices, per-point
+//     contribution lists, dependency list; built by plan.cu) into one of four
+//     record slots with a bulk copy on the TMA engine (no multicast).  Once
+//     the compute threads have written a tile back it refills the tile's slot
+//     with the tile four places ahead and publishes the tile's completion
+//     flag (per block: iterations completed, counted from Ctl::base);
+//   * the STAGING warp gathers a tile's read rows into one of two row slots
+//     with cp.async, then polls the completion flags of the blocks the tile
+//     conflicts with and, once they hold, prefetches the tile's output rows;
+//   * the COMPUTE threads compute each cell's per-slot increments into
+//     shared memory, then, per written point, sum its contributions in
+//     thread-colour order -- the order of the reference's colour-by-colour
+//     shared accumulation, so results stay bit-identical to the CPU replay --
+//     and store out[p] + sum.
+// The roles hand over through mbarriers (record landed, rows landed, output
+// rows landed / dependencies held, tile written back); the compute threads
+// also meet at a named barrier three times per tile.  The claim, the record
+// copy and the flag release therefore stay off the compute threads' path.
+// Every wait is bounded: after about two seconds the kernel sets
+// kErrWaitLimit in Ctl::error, drains its copies in flight and returns.
 #pragma once
 
 #include <cstdint>
@@ -57,33 +64,66 @@ template <class L> struct RecView {
   }
 };
 
+// ---- small PTX helpers of the warp-specialised kernel -------------------------
 __device__ __forceinline__ unsigned int ld_relaxed_gpu(const unsigned int *p) {
   unsigned int v;
   asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ void fence_acq_rel_gpu() {
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+// arrive once every cp.async this thread issued so far has landed
+__device__ __forceinline__ void mbar_arrive_cp_async(uint64_t *bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+template <int T> __device__ __forceinline__ void named_bar_sync() {
+  asm volatile("bar.sync 1, %0;" ::"n"(T) : "memory");
+}
+// named barrier 1 over T threads that also ANDs a predicate
+template <int T> __device__ __forceinline__ bool named_bar_and(bool v) {
+  unsigned r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.and.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}"
+      : "=r"(r)
+      : "r"((unsigned)v), "n"(T)
+      : "memory");
+  return r != 0;
+}
+// Bounded mbarrier wait that also gives up once *stop is set.
+__device__ __forceinline__ bool mbar_wait_or_stop(uint64_t *bar, unsigned phase,
+                                                  const volatile uint32_t *stop) {
+  if (mbar_try_wait(bar, phase)) return true;
+  const uint64_t t0 = global_timer_ns();
+  for (unsigned i = 1;; ++i) {
+    if (mbar_try_wait(bar, phase)) return true;
+    if ((i & 15u) == 0 && (*stop || global_timer_ns() - t0 > 2000000000ull)) return false;
+  }
+}
 
-// Dependency flags of a tile, read by the lanes of one warp: every block
-// conflicting with the tile must have completed what precedes it -- blocks
-// of an earlier colour iteration `it` (flag >= it + 1), the others and the
-// block itself iteration it - 1 (flag >= it); `it` counts from the launch's
-// base.  Lane l holds entries l, l + 32, ... (up to kDepPerLane of them);
-// the block's own flag is the entry after the list.
+// Dependency flags of a tile, read by the 32 lanes of one warp: every block
+// conflicting with the tile must have completed what precedes it -- blocks of
+// an earlier colour iteration `it` (flag >= it + 1), the others and the block
+// itself iteration it - 1 (flag >= it); `it` counts from Ctl::base.  Lane l
+// holds entries l, l + 32, ...; the block's own flag is the entry after the
+// list.  Loads are relaxed; the caller issues one acquire fence once all hold.
 constexpr int kDepPerLane = 4;
 
-template <class L> struct DepProbe {
+struct DepProbe {
   unsigned int have[kDepPerLane];
   unsigned int need[kDepPerLane];
   const unsigned int *ptr[kDepPerLane];
-  bool overflow;
 
-  // issue relaxed loads (non-blocking until evaluated)
-  __device__ __forceinline__ void issue(const RecView<L> &m, uint32_t it, const unsigned int *flags) {
+  template <class L>
+  __device__ __forceinline__ void issue(const RecView<L> &m, uint32_t it, const unsigned int *flags,
+                                        uint32_t round) {
     const uint32_t lane = threadIdx.x & 31u;
-    overflow = m.ndep + 1 > 32u * kDepPerLane;
 #pragma unroll
     for (int q = 0; q < kDepPerLane; ++q) {
-      const uint32_t e = lane + 32u * q;
+      const uint32_t e = lane + 32u * (q + kDepPerLane * round);
       ptr[q] = nullptr;
       need[q] = 0;
       have[q] = 0;
@@ -102,14 +142,12 @@ template <class L> struct DepProbe {
       }
     }
   }
-  // all satisfied (warp-uniform)
-  __device__ __forceinline__ bool ready() const {
-    bool ok = !overflow;
+  __device__ __forceinline__ bool ready() const {  // warp-uniform
+    bool ok = true;
 #pragma unroll
     for (int q = 0; q < kDepPerLane; ++q) ok = ok && have[q] >= need[q];
     return __all_sync(0xFFFFFFFFu, ok);
   }
-  // re-read the flags not yet satisfied
   __device__ __forceinline__ void reload() {
 #pragma unroll
     for (int q = 0; q < kDepPerLane; ++q)
@@ -117,33 +155,35 @@ template <class L> struct DepProbe {
   }
 };
 
-// Blocking bounded check for a tile whose list is too long for a probe.
+// Wait (bounded by wall time) until every dependency of a tile holds; all
+// 32 lanes of the warp call it.  Returns false on timeout or stop.
 template <class L>
-__device__ __forceinline__ bool deps_ready_slow(const RecView<L> &m, uint32_t it,
-                                                const unsigned int *flags) {
-  const uint32_t lane = threadIdx.x & 31u;
-  bool ok = true;
-  for (uint32_t e = lane; e <= m.ndep; e += 32) {
-    uint32_t blk, need;
-    if (e == m.ndep) {
-      blk = m.block;
-      need = it;
-    } else {
-      const uint32_t v = m.dep[e];
-      blk = v & 0x7FFFFFFFu;
-      need = it + (v >> 31);
+__device__ __forceinline__ bool wait_deps(const RecView<L> &m, uint32_t it, const unsigned int *flags,
+                                          const volatile uint32_t *stop) {
+  const uint32_t rounds = (m.ndep + 1 + 32u * kDepPerLane - 1) / (32u * kDepPerLane);
+  uint64_t t0 = 0;
+  for (uint32_t r = 0; r < rounds; ++r) {
+    DepProbe pr;
+    pr.issue(m, it, flags, r);
+    for (unsigned i = 0; !pr.ready(); ++i) {
+      if ((i & 15u) == 0) {
+        const uint64_t t = global_timer_ns();
+        if (t0 == 0) t0 = t;
+        if (*stop || t - t0 > 2000000000ull) return false;
+      }
+      __nanosleep(64);
+      pr.reload();
     }
-    if (ld_acquire_gpu(flags + blk) < need) ok = false;
   }
-  return __all_sync(0xFFFFFFFFu, ok);
+  return true;
 }
 
-// Stage the read rows of a tile (points from its record) into buffer `buf`.
-template <class L, bool SOA, int THREADS>
-__device__ __forceinline__ void pipe_stage_rows(const LoopData &d, const HierPlanDev &P,
-                                                unsigned char *buf, const RecView<L> &m) {
+// Stage the read rows of a tile into a row slot: the 32 lanes of one warp.
+template <class L, bool SOA>
+__device__ __forceinline__ void ws_stage_rows(const LoopData &d, const HierPlanDev &P,
+                                              unsigned char *slot, const RecView<L> &m) {
   using read_t = typename L::read_t;
-  const uint32_t tid = threadIdx.x;
+  const uint32_t lane = threadIdx.x & 31u;
   static_for_read<L>([&](auto r) {
     constexpr int R = decltype(r)::value;
     constexpr int DIM = L::read_dim(R);
@@ -152,11 +192,11 @@ __device__ __forceinline__ void pipe_stage_rows(const LoopData &d, const HierPla
     const uint32_t n = c0 ? m.n0 : m.n1;
     const uint32_t *pts = c0 ? m.pts0 : m.pts1;
     const char *src = static_cast<const char *>(d.point[L::read_set(R)]);
-    char *dst = reinterpret_cast<char *>(buf + P.read_off[R]);
+    char *dst = reinterpret_cast<char *>(slot + P.read_off[R]);
     if constexpr (!SOA) {
       constexpr int CS = ROW % 16 == 0 ? 16 : (ROW % 8 == 0 ? 8 : 4);
       constexpr int CH = ROW / CS;
-      for (uint32_t e = tid; e < n * CH; e += THREADS) {
+      for (uint32_t e = lane; e < n * CH; e += 32) {
         const uint32_t i = e / CH, c = e - i * CH;
         const char *g = src + (size_t)pts[i] * ROW + c * CS;
         char *s = dst + (size_t)i * ROW + c * CS;
@@ -166,7 +206,7 @@ __device__ __forceinline__ void pipe_stage_rows(const LoopData &d, const HierPla
       }
     } else {
       const uint32_t np = d.n_points[L::read_set(R)];
-      for (uint32_t e = tid; e < n * DIM; e += THREADS) {
+      for (uint32_t e = lane; e < n * DIM; e += 32) {
         const uint32_t k = e / n, i = e - k * n;
         const char *g = src + ((size_t)k * np + pts[i]) * sizeof(read_t);
         char *s = dst + ((size_t)i * DIM + k) * sizeof(read_t);
@@ -177,236 +217,260 @@ __device__ __forceinline__ void pipe_stage_rows(const LoopData &d, const HierPla
   });
 }
 
-template <class L, bool SOA, int THREADS>
-__global__ void __launch_bounds__(THREADS, hier_min_blocks<L, THREADS>())
+// Resident CTAs per SM the kernel's register cap aims for (T + 64 threads).
+template <class L, int T> constexpr int ws_min_blocks() {
+  return (65536 / ((T + 64) * L::kRegCap)) > 0 ? 65536 / ((T + 64) * L::kRegCap) : 1;
+}
+
+constexpr uint32_t kRecSlots = 4;
+
+template <class L, bool SOA, int T>
+__global__ void __launch_bounds__(T + 64, ws_min_blocks<L, T>())
     k_hier_pipe(LoopData d, HierPlanDev P) {
   using out_t = typename L::out_t;
   using read_t = typename L::read_t;
   constexpr int D = L::kDim, K = L::kOut;
   constexpr int ROW_OUT = K * (int)sizeof(out_t);
   constexpr bool kPrefetchOut = !SOA && ROW_OUT % 16 == 0;
-  constexpr uint32_t NONE = 0xFFFFFFFFu;
+  constexpr uint32_t kRecordWarp = T / 32, kStagingWarp = T / 32 + 1;
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ __align__(8) uint64_t s_bar[2];
-  __shared__ uint32_t s_iter[2];
-  __shared__ uint32_t s_valid[2];
-  __shared__ int s_dep[2];  // the dependencies of the tile in each buffer already held
-  __shared__ int s_abort;
+  __shared__ __align__(8) uint64_t s_rec_full[kRecSlots];
+  __shared__ __align__(8) uint64_t s_tile_done[kRecSlots];
+  __shared__ __align__(8) uint64_t s_rows_full[2];
+  __shared__ __align__(8) uint64_t s_out_full[2];
+  __shared__ uint32_t s_iter[kRecSlots];   // iteration of the tile in each record slot
+  __shared__ uint32_t s_valid[kRecSlots];  // 0: no tile (end of this CTA's queue)
+  __shared__ uint32_t s_abort[2];          // per row slot: skip the write-back
+  __shared__ volatile uint32_t s_stop;     // a role gave up (error path)
   const uint32_t tid = threadIdx.x;
-  out_t *inc = reinterpret_cast<out_t *>(smem + P.inc_off);
-  out_t *outbuf = reinterpret_cast<out_t *>(smem + P.outbuf_off);
+  const uint32_t warp = tid >> 5, lane = tid & 31u;
+  unsigned char *const rec_base = smem;
+  unsigned char *const rows_base = smem + P.rows_off;
+  out_t *const inc = reinterpret_cast<out_t *>(smem + P.inc_off);
   out_t *__restrict__ out = static_cast<out_t *>(d.out);
+
+  if (tid == 0) {
+    for (uint32_t s = 0; s < kRecSlots; ++s) {
+      mbar_init(&s_rec_full[s], 1);
+      mbar_init(&s_tile_done[s], T / 32);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&s_rows_full[b], 33);
+      mbar_init(&s_out_full[b], 33);
+    }
+    mbar_fence_init();
+    s_stop = 0;
+  }
+  __syncthreads();
   const uint32_t base = *(volatile unsigned int *)&P.ctl->base;
 
-  // thread 0's pipeline state
-  uint32_t t_claim = NONE;                     // ticket for the next buffer refill
-  uint32_t pre_off = 0, pre_bytes = 0, pre_iter = 0;  // its record
-  bool pre_ok = false;
-
-  auto claim = [&]() {  // thread 0
-    t_claim = atomicAdd(&P.ctl->ticket, 1u);
-  };
-  auto prefetch_record_info = [&]() {  // thread 0, after claim()
-    pre_ok = t_claim < P.total_tiles && !(*(volatile unsigned int *)&P.ctl->error);
-    if (pre_ok) {
-      const uint32_t it = t_claim / P.n_blocks, b = t_claim - it * P.n_blocks;
-      pre_off = P.rec_off[b];
-      pre_bytes = P.rec_off[b + 1] - pre_off;
-      pre_iter = it;
-    }
-  };
-  auto issue_record = [&](int c) {  // thread 0: refill buffer c with the claimed tile
-    if (pre_ok) {
-      s_iter[c] = pre_iter;
-      s_valid[c] = 1;
-      // the buffer was last read through the generic proxy
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_expect_tx(&s_bar[c], pre_bytes);
-      bulk_copy_g2s(smem + c * P.buf_bytes, P.rec + pre_off, pre_bytes, &s_bar[c]);
-    } else {
-      s_valid[c] = 0;
-    }
-  };
-
-  if (tid == 0) {
-    mbar_init(&s_bar[0], 1);
-    mbar_init(&s_bar[1], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-  if (tid == 0) {
-    claim();
-    prefetch_record_info();
-    issue_record(0);
-    claim();
-    prefetch_record_info();
-    issue_record(1);
-    claim();
-  }
-  __syncthreads();
-  {
-    const bool first = s_valid[0];
-    const bool ok = !first || mbar_wait(&s_bar[0], 0);
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) {
-        atomicOr(&P.ctl->error, kErrWaitLimit);
-        s_valid[0] = 0;
+  if (warp == kRecordWarp) {
+    // ---------------------------------------------------------------- record
+    if (lane == 0) {
+      uint32_t uses[kRecSlots] = {0, 0, 0, 0};  // copies issued per slot
+      bool valid[kRecSlots] = {false, false, false, false};
+      uint32_t blk[kRecSlots] = {0, 0, 0, 0};
+      // claim pipeline: ticket t_a with its record offsets loaded, ticket t_b
+      // claimed one refill earlier
+      uint32_t t_a = atomicAdd(&P.ctl->ticket, 1u);
+      uint32_t t_b = atomicAdd(&P.ctl->ticket, 1u);
+      uint32_t a_off = 0, a_end = 0, a_err = 0;
+      auto load_a = [&]() {
+        if (t_a < P.total_tiles) {
+          const uint32_t b = t_a % P.n_blocks;
+          a_off = P.rec_off[b];
+          a_end = P.rec_off[b + 1];
+        }
+        a_err = *(volatile unsigned int *)&P.ctl->error;
+      };
+      bool more = true;
+      auto refill = [&](uint32_t s) {  // slot s gets ticket t_a
+        const bool ok = more && t_a < P.total_tiles && a_err == 0;
+        const uint32_t it = ok ? t_a / P.n_blocks : 0;
+        s_iter[s] = it;
+        s_valid[s] = ok;
+        valid[s] = ok;
+        blk[s] = ok ? t_a - it * P.n_blocks : 0;
+        if (ok) {
+          // the slot was last read through the generic proxy
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          mbar_expect_tx(&s_rec_full[s], a_end - a_off);
+          bulk_copy_g2s(rec_base + s * P.rec_slot, P.rec + a_off, a_end - a_off, &s_rec_full[s]);
+        } else {
+          mbar_arrive(&s_rec_full[s]);
+          more = false;
+        }
+        ++uses[s];
+        t_a = t_b;
+        if (more) {
+          load_a();
+          t_b = atomicAdd(&P.ctl->ticket, 1u);
+        }
+      };
+      load_a();
+      for (uint32_t s = 0; s < kRecSlots && more; ++s) refill(s);
+      for (uint32_t j = 0;; ++j) {
+        const uint32_t s = j % kRecSlots;
+        if (!valid[s]) break;
+        if (!mbar_wait_or_stop(&s_tile_done[s], (j / kRecSlots) & 1u, &s_stop)) {
+          atomicOr(&P.ctl->error, kErrWaitLimit);
+          s_stop = 1;
+          break;
+        }
+        const uint32_t done_block = blk[s], done_it = base + s_iter[s] + 1;
+        if (more) refill(s);
+        else valid[s] = false;
+        // the compute threads' stores (ordered before this thread by the
+        // mbarrier) become visible before the flag
+        st_release_gpu(P.block_done + done_block, done_it);
       }
-      __syncthreads();
-    } else if (first) {
-      const RecView<L> m0(smem);
-      pipe_stage_rows<L, SOA, THREADS>(d, P, smem, m0);
-      if (tid < 32) {
-        const bool r = deps_ready_slow(m0, base + s_iter[0], P.block_done);
-        if (tid == 0) s_dep[0] = r;
-      }
+      // let every record copy still in flight land (bounded)
+      for (uint32_t s = 0; s < kRecSlots; ++s)
+        if (uses[s] > 0) (void)mbar_wait(&s_rec_full[s], (uses[s] - 1) & 1u);
     }
-  }
-  cp_async_commit();
-
-  for (uint32_t k = 0;; ++k) {
-    const int c = k & 1, n = c ^ 1;
-    if (!s_valid[c]) break;
-    unsigned char *buf = smem + c * P.buf_bytes;
-    const RecView<L> m(buf);
-    const uint32_t iter = s_iter[c];
-    const uint32_t it_abs = base + iter;
-    // 1. the claimed tile's record offsets
-    if (tid == 0) prefetch_record_info();
-    // 2. this tile's rows have landed
-    cp_async_wait_group<0>();
-    __syncthreads();
-    // 3. prefetch this tile's output rows when its dependencies already held
-    //    (checked when its record arrived)
-    const bool dep = s_dep[c];
-    if constexpr (kPrefetchOut) {
-      if (dep) {
+    __syncwarp();
+  } else if (warp == kStagingWarp) {
+    // --------------------------------------------------------------- staging
+    bool err = false;
+    for (uint32_t j = 0;; ++j) {
+      const uint32_t s = j % kRecSlots, b = j & 1u;
+      bool ok = mbar_wait_or_stop(&s_rec_full[s], (j / kRecSlots) & 1u, &s_stop);
+      // the row slot and output slot of tile j - 2 are free once it is written back
+      if (ok && j >= 2)
+        ok = mbar_wait_or_stop(&s_tile_done[(j - 2) % kRecSlots], ((j - 2) / kRecSlots) & 1u, &s_stop);
+      ok = __all_sync(0xFFFFFFFFu, ok);
+      if (!ok || err || !s_valid[s]) {
+        if (!ok && !err) {
+          err = true;
+          if (lane == 0) atomicOr(&P.ctl->error, kErrWaitLimit);
+        }
+        if (lane == 0) {
+          s_valid[s] = 0;
+          if (err) s_stop = 1;
+          mbar_arrive(&s_rows_full[b]);
+        }
+        mbar_arrive(&s_rows_full[b]);
+        break;
+      }
+      const RecView<L> m(rec_base + s * P.rec_slot);
+      ws_stage_rows<L, SOA>(d, P, rows_base + b * P.rows_bytes, m);
+      mbar_arrive_cp_async(&s_rows_full[b]);
+      if (lane == 0) mbar_arrive(&s_rows_full[b]);
+      // dependencies, then the output rows
+      const bool dep_ok = wait_deps(m, base + s_iter[s], P.block_done, &s_stop);
+      fence_acq_rel_gpu();
+      if (kPrefetchOut && dep_ok) {
         constexpr int CH = ROW_OUT / 16;
-        char *ob = reinterpret_cast<char *>(outbuf);
+        char *ob = reinterpret_cast<char *>(smem + P.outbuf_off + b * P.outbuf_bytes);
         const char *og = reinterpret_cast<const char *>(out);
-        for (uint32_t e = tid; e < m.n0 * CH; e += THREADS) {
+        for (uint32_t e = lane; e < m.n0 * CH; e += 32) {
           const uint32_t i = e / CH, q = e - i * CH;
           cp_async16(ob + (size_t)i * ROW_OUT + q * 16, og + (size_t)m.pts0[i] * ROW_OUT + q * 16);
         }
       }
+      if (lane == 0) {
+        s_abort[b] = dep_ok ? 0u : 1u;
+        if (!dep_ok) atomicOr(&P.ctl->error, kErrWaitLimit);
+      }
+      mbar_arrive_cp_async(&s_out_full[b]);
+      if (lane == 0) mbar_arrive(&s_out_full[b]);
+      if (!dep_ok) err = true;  // later tiles are dropped
     }
-    cp_async_commit();
-    // 4. the next tile's record, then its rows (a record that did not arrive
-    //    in time ends this CTA's queue after the current tile)
-    {
-      const bool next = s_valid[n];
-      const bool ok = !next || mbar_wait(&s_bar[n], ((k + 1) >> 1) & 1u);
-      if (__syncthreads_or(!ok)) {
+    cp_async_wait_all();
+  } else {
+    // --------------------------------------------------------------- compute
+    for (uint32_t j = 0;; ++j) {
+      const uint32_t s = j % kRecSlots, b = j & 1u, ph = (j >> 1) & 1u;
+      const bool ok_rows = mbar_wait_or_stop(&s_rows_full[b], ph, &s_stop);
+      if (!named_bar_and<T>(ok_rows)) {
         if (tid == 0) {
           atomicOr(&P.ctl->error, kErrWaitLimit);
-          s_valid[n] = 0;
+          s_stop = 1;
         }
-      } else if (next) {
-        const RecView<L> mn(smem + n * P.buf_bytes);
-        pipe_stage_rows<L, SOA, THREADS>(d, P, smem + n * P.buf_bytes, mn);
-        // the next tile's dependencies (read now, used when it starts)
-        if (tid < 32) {
-          const bool r = deps_ready_slow(mn, base + s_iter[n], P.block_done);
-          if (tid == 0) s_dep[n] = r;
+        break;
+      }
+      if (!s_valid[s]) break;
+      // the record landed through the async proxy
+      (void)mbar_try_wait(&s_rec_full[s], (j / kRecSlots) & 1u);
+      const RecView<L> m(rec_base + s * P.rec_slot);
+      const unsigned char *rows = rows_base + b * P.rows_bytes;
+      if (tid < m.ncell) {
+        SmemRows<L> rv;
+#pragma unroll
+        for (int q = 0; q < D; ++q) {
+          rv.l[0][q] = m.lidx0[q * m.ncell + tid];
+          rv.l[1][q] = L::kHasClass1 ? m.lidx1[q * m.ncell + tid] : 0;
         }
+        static_for_read<L>([&](auto r) {
+          constexpr int R = decltype(r)::value;
+          rv.base[R] = reinterpret_cast<const read_t *>(rows + P.read_off[R]);
+        });
+        out_t v[D][K];
+        Direct dir{d.cell, m.start + tid, d.n_cells};
+        L::cell(rv, dir, v);
+#pragma unroll
+        for (int q = 0; q < D; ++q)
+#pragma unroll
+          for (int k = 0; k < K; ++k) inc[(k * D + q) * T + tid] = v[q][k];
       }
-    }
-    cp_async_commit();
-    // 5. compute: per-slot increments of each cell into the shared buffer
-    if (tid < m.ncell) {
-      SmemRows<L> rows;
+      named_bar_sync<T>();
+      const bool ok_out = mbar_wait_or_stop(&s_out_full[b], ph, &s_stop);
+      if (ok_out && !s_abort[b]) {
+        const out_t *ob = reinterpret_cast<const out_t *>(smem + P.outbuf_off + b * P.outbuf_bytes);
+        for (uint32_t i = tid; i < m.n0; i += T) {
+          out_t acc[K];
 #pragma unroll
-      for (int s = 0; s < D; ++s) {
-        rows.l[0][s] = m.lidx0[s * m.ncell + tid];
-        rows.l[1][s] = L::kHasClass1 ? m.lidx1[s * m.ncell + tid] : 0;
-      }
-      static_for_read<L>([&](auto r) {
-        constexpr int R = decltype(r)::value;
-        rows.base[R] = reinterpret_cast<const read_t *>(buf + P.read_off[R]);
-      });
-      out_t v[D][K];
-      Direct dir{d.cell, m.start + tid, d.n_cells};
-      L::cell(rows, dir, v);
+          for (int k = 0; k < K; ++k) acc[k] = out_t(0);
+          const uint32_t e0 = m.pc_off[i], e1 = m.pc_off[i + 1];
+          for (uint32_t e = e0; e < e1; ++e) {
+            const uint32_t ie = m.pc_idx[e];
 #pragma unroll
-      for (int s = 0; s < D; ++s)
-#pragma unroll
-        for (int q = 0; q < K; ++q) inc[(q * D + s) * THREADS + tid] = v[s][q];
-    }
-    // 6. output rows (if prefetched) landed; otherwise wait (bounded) for the
-    //    dependencies
-    cp_async_wait_group<1>();
-    if (tid < 32) {
-      int ab = 0;
-      if (!dep) {
-        unsigned int polls = 0;
-        while (!deps_ready_slow(m, it_abs, P.block_done)) {
-          if (++polls > kWaitPollLimit) {
-            if (tid == 0) atomicOr(&P.ctl->error, kErrWaitLimit);
-            ab = 1;
-            break;
+            for (int k = 0; k < K; ++k) acc[k] += inc[k * D * T + ie];
           }
-          __nanosleep(128);
-        }
-      }
-      if (tid == 0) s_abort = ab;
-    }
-    __syncthreads();
-    // 7. per written point: sum its contributions in thread-colour order and
-    //    add to the output row
-    if (!s_abort) {
-      for (uint32_t j = tid; j < m.n0; j += THREADS) {
-        out_t acc[K];
+          const uint32_t p = m.pts0[i];
+          if constexpr (kPrefetchOut) {
+            using vec_t = typename std::conditional<sizeof(out_t) == 8, double2, float4>::type;
+            constexpr int CH = ROW_OUT / 16;
+            constexpr int PER = 16 / sizeof(out_t);
+            vec_t *og = reinterpret_cast<vec_t *>(out) + (size_t)p * CH;
+            const vec_t *obv = reinterpret_cast<const vec_t *>(ob) + (size_t)i * CH;
 #pragma unroll
-        for (int q = 0; q < K; ++q) acc[q] = out_t(0);
-        const uint32_t e0 = m.pc_off[j], e1 = m.pc_off[j + 1];
-        for (uint32_t e = e0; e < e1; ++e) {
-          const uint32_t ie = m.pc_idx[e];
-#pragma unroll
-          for (int q = 0; q < K; ++q) acc[q] += inc[q * D * THREADS + ie];
-        }
-        const uint32_t p = m.pts0[j];
-        if constexpr (kPrefetchOut) {
-          using vec_t = typename std::conditional<sizeof(out_t) == 8, double2, float4>::type;
-          constexpr int CH = ROW_OUT / 16;
-          constexpr int PER = 16 / sizeof(out_t);
-          vec_t *og = reinterpret_cast<vec_t *>(out) + (size_t)p * CH;
-          const vec_t *ob = reinterpret_cast<const vec_t *>(outbuf) + (size_t)j * CH;
-#pragma unroll
-          for (int q = 0; q < CH; ++q) {
-            vec_t w = dep ? ob[q] : __ldcg(og + q);
-            if constexpr (PER == 2) {
-              w.x += acc[q * 2];
-              w.y += acc[q * 2 + 1];
-            } else {
-              w.x += acc[q * 4];
-              w.y += acc[q * 4 + 1];
-              w.z += acc[q * 4 + 2];
-              w.w += acc[q * 4 + 3];
+            for (int q = 0; q < CH; ++q) {
+              vec_t w = obv[q];
+              if constexpr (PER == 2) {
+                w.x += acc[q * 2];
+                w.y += acc[q * 2 + 1];
+              } else {
+                w.x += acc[q * 4];
+                w.y += acc[q * 4 + 1];
+                w.z += acc[q * 4 + 2];
+                w.w += acc[q * 4 + 3];
+              }
+              __stcg(og + q, w);
             }
-            __stcg(og + q, w);
+          } else {
+            out_t o[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) o[k] = __ldcg(out + out_index(SOA, d.n_points[0], p, K, k));
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+              __stcg(out + out_index(SOA, d.n_points[0], p, K, k), o[k] + acc[k]);
           }
-        } else {
-          out_t o[K];
-#pragma unroll
-          for (int q = 0; q < K; ++q) o[q] = __ldcg(out + out_index(SOA, d.n_points[0], p, K, q));
-#pragma unroll
-          for (int q = 0; q < K; ++q) __stcg(out + out_index(SOA, d.n_points[0], p, K, q), o[q] + acc[q]);
         }
       }
-    }
-    __syncthreads();
-    // 8. signal; refill this buffer with the claimed tile; claim the next
-    if (tid == 0) {
-      st_release_gpu(P.block_done + m.block, it_abs + 1);
-      issue_record(c);
-      if (pre_ok) claim();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&s_tile_done[s]);
+      // the increments buffer is reused by the next tile
+      if (!named_bar_and<T>(ok_out)) {
+        if (tid == 0) {
+          atomicOr(&P.ctl->error, kErrWaitLimit);
+          s_stop = 1;
+        }
+        break;
+      }
     }
   }
-  // after an error, let any record copy still in flight land (bounded)
-  if (tid == 0 && *(volatile unsigned int *)&P.ctl->error)
-    for (int c = 0; c < 2; ++c)
-      if (!mbar_try_wait(&s_bar[c], 0) || !mbar_try_wait(&s_bar[c], 1))
-        (void)(mbar_wait(&s_bar[c], 0) && mbar_wait(&s_bar[c], 1));
+  __syncthreads();
   // the last CTA to leave resets the queue and advances the flags' base by
   // the iterations of this launch
   if (tid == 0) {

@@ -46,7 +46,6 @@ template <bool SOA> const void *pipe_kernel(uint32_t threads) {
   case 128: return reinterpret_cast<const void *>(&k_hier_pipe<L, SOA, 128>);
   case 256: return reinterpret_cast<const void *>(&k_hier_pipe<L, SOA, 256>);
   case 512: return reinterpret_cast<const void *>(&k_hier_pipe<L, SOA, 512>);
-  case 1024: return reinterpret_cast<const void *>(&k_hier_pipe<L, SOA, 1024>);
   }
   return nullptr;
 }
@@ -77,7 +76,8 @@ int run_hier(const LoopData &d, const HierPlanDev &P, bool soa, uint32_t threads
   if (!k) return fail(FOT_ERR_ARG, "no hierarchical kernel for %u threads", threads);
   FOT_TRY(prepare(k, smem));
   void *args[] = {const_cast<LoopData *>(&d), const_cast<HierPlanDev *>(&P)};
-  FOT_CUDA(cudaLaunchKernel(k, dim3(grid), dim3(threads), args, smem, st));
+  const uint32_t block = (variant & kVariantPipe) ? threads + 64 : threads;
+  FOT_CUDA(cudaLaunchKernel(k, dim3(grid), dim3(block), args, smem, st));
   return FOT_OK;
 }
 
@@ -96,8 +96,9 @@ int occupancy(int exec, bool soa, uint32_t threads, uint32_t variant, size_t sme
   const void *k = kernel_for(exec, soa, exec == FOT_EXEC_ATOMIC ? 256 : threads, variant);
   if (!k) return fail(FOT_ERR_ARG, "no kernel for %u threads", threads);
   if (exec != FOT_EXEC_ATOMIC) FOT_TRY(prepare(k, smem));
-  FOT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      per_sm, k, exec == FOT_EXEC_ATOMIC ? 256 : (int)threads, smem));
+  int block = exec == FOT_EXEC_ATOMIC ? 256 : (int)threads;
+  if (exec == FOT_EXEC_HIER && (variant & kVariantPipe)) block += 64;
+  FOT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k, block, smem));
   return FOT_OK;
 }
 
@@ -110,20 +111,27 @@ void smem_layout(uint32_t cap0, uint32_t cap1, uint32_t variant, uint32_t rec_ca
   SmemLayout s;
   size_t off = 0;
   if (variant & kVariantPipe) {
-    // buffer = [tile record][read rows]; two buffers, then the increments and
-    // the prefetched output rows
-    off = a16(rec_cap);
+    // 4 tile-record slots, 2 read-row slots, the per-slot increments, 2
+    // prefetched-output-row slots (AOS output rows of a multiple of 16 bytes)
+    auto a128 = [](size_t v) { return (v + 127) & ~size_t(127); };
+    s.rec_slot = (uint32_t)a128(rec_cap);
+    off = 4 * (size_t)s.rec_slot;
+    s.rows_off = (uint32_t)off;
+    size_t rows = 0;
     for (int r = 0; r < L::kNumRead; ++r) {
-      s.read_off[r] = (uint32_t)off;
+      s.read_off[r] = (uint32_t)rows;
       const uint32_t cap = L::read_class(r) == 0 ? cap0 : cap1;
-      off = a16(off + (size_t)cap * L::read_dim(r) * sizeof(read_t));
+      rows = a16(rows + (size_t)cap * L::read_dim(r) * sizeof(read_t));
     }
-    s.buf_bytes = (uint32_t)((off + 127) & ~size_t(127));
-    off = 2 * (size_t)s.buf_bytes;
+    s.rows_bytes = (uint32_t)a128(rows);
+    off += 2 * (size_t)s.rows_bytes;
     s.inc_off = (uint32_t)off;
-    off = a16(off + (size_t)L::kOut * L::kDim * threads * sizeof(out_t));
+    off = a128(off + (size_t)L::kOut * L::kDim * threads * sizeof(out_t));
     s.outbuf_off = (uint32_t)off;
-    if ((L::kOut * sizeof(out_t)) % 16 == 0) off = a16(off + (size_t)cap0 * L::kOut * sizeof(out_t));
+    if ((L::kOut * sizeof(out_t)) % 16 == 0) {
+      s.outbuf_bytes = (uint32_t)a128((size_t)cap0 * L::kOut * sizeof(out_t));
+      off += 2 * (size_t)s.outbuf_bytes;
+    }
     s.total = off;
     *out = s;
     return;
