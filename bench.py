@@ -45,18 +45,20 @@ def load_peaks():
 
 
 def load_traffic(kernel_key):
-    """Per-launch DRAM traffic of the dominant kernel from the committed ncu
-    summary (profiles/traffic.json), or None."""
+    """Per-launch DRAM traffic (bytes) of the dominant kernel and where it
+    comes from, from the committed ncu summary (profiles/traffic.json)."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             j = json.load(f)
-        return j.get(kernel_key)
+        e = j[kernel_key]
+        return float(e["bytes_per_launch"]), e.get("source")
     except Exception:
-        return None
+        return None, None
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons, sampled every 100 ms by one
+    `nvidia-smi -lms` process that runs across the timed region."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -65,30 +67,38 @@ class ClockSampler:
     def __init__(self, index=0):
         self.index = index
         self.rows = []
-        self._stop = threading.Event()
+        self._proc = None
         self._t = None
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(
-                    ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                     "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                if out.returncode == 0 and out.stdout.strip():
-                    self.rows.append([v.strip() for v in out.stdout.strip().split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        for line in self._proc.stdout:
+            v = [x.strip() for x in line.strip().split(",")]
+            if len(v) >= 7:
+                self.rows.append(v)
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+            time.sleep(0.3)  # first sample before the timed region starts
+        except Exception:
+            self._proc = None
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        if self._t:
-            self._t.join(timeout=10)
+        if self._proc is not None:
+            time.sleep(0.15)
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+            if self._t:
+                self._t.join(timeout=5)
 
     def summary(self):
         if not self.rows:
@@ -173,20 +183,30 @@ def run_reference(args):
         kind = "reference"
         for _ in range(max(0, min(args.warmup, 1))):
             O.ref_omp(md, 1)
+        # steps are timed until about 90 s of host time are spent, so the
+        # default step count finishes within minutes
         times = []
+        t_wall = time.perf_counter()
         for _ in range(args.steps):
             _, _, t_loop, _ = O.ref_omp(md, 1)
             times.append(t_loop)
+            if time.perf_counter() - t_wall > 90.0:
+                break
         secs = sum(times) / len(times)
-        sample = "loopCPUCellCentredOMP, 1 iteration of the full mesh per step (colouring excluded)"
+        sample = (f"loopCPUCellCentredOMP, 1 iteration of the full mesh per step (colouring "
+                  f"excluded), {len(times)} of {args.steps} steps timed (90 s host-time cap)")
     else:
         kind = "port"
         t0 = time.perf_counter()
+        n = 0
         for _ in range(args.steps):
             O.serial(md, 1)
-        secs = (time.perf_counter() - t0) / args.steps
+            n += 1
+            if time.perf_counter() - t0 > 90.0:
+                break
+        secs = (time.perf_counter() - t0) / n
         cores = 1
-        sample = "oracle serial loop, 1 iteration of the full mesh per step"
+        sample = f"oracle serial loop, 1 iteration of the full mesh per step, {n} of {args.steps} steps timed"
     v = ub / secs / 1e9
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3,
@@ -203,7 +223,7 @@ def run_reference(args):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=600)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="fot", choices=["fot", "reference"])
     ap.add_argument("--n", type=int, default=128)
@@ -312,7 +332,7 @@ def main(argv=None):
     peak, peak_src = load_peaks()
     achieved = ub / per_launch / 1e9 if launches_per_step == 1 else ub / (secs / args.steps) / 1e9
     kernel_key = f"{chosen.exec}"
-    traffic = load_traffic(kernel_key)
+    traffic, traffic_src = load_traffic(kernel_key)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(md)
@@ -336,7 +356,8 @@ def main(argv=None):
             "speedup_vs_atomic": (value / world) / atomic_plain["gbs"] if atomic_plain.get("ok") else None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_src,
-                         "traffic": traffic},
+                         "traffic": traffic, "traffic_unit": "bytes per launch",
+                         "traffic_source": traffic_src},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
