@@ -38,7 +38,8 @@ FEATURES = [
     "loop_res_calc", "loop_mini_aero", "loop_lulesh", "loop_volna", "loop_getacc",
     "deg_le2", "deg_3_4", "deg_5_6", "deg_ge7",
     "log10_1p_bandwidth", "log10_1p_mean_span",
-    "exec_atomic", "exec_hier", "exec_hier_launch", "log2_block", "partitioned", "direct_reads",
+    "exec_atomic", "exec_hier", "exec_hier_launch", "log2_block", "partitioned",
+    "direct_reads_or_plain_atomics",
 ]
 assert len(FEATURES) == N_FEATURES
 
@@ -76,10 +77,15 @@ def mesh_features(md: mg.MeshData) -> np.ndarray:
 
 
 def plan_features(c: T.Candidate) -> np.ndarray:
+    """7 plan features; the last one is 1 for direct (unstaged) reads of a
+    hierarchical plan and for an atomic plan without warp aggregation."""
     ex = np.zeros(3)
     ex[["atomic", "hier", "hier_launch"].index(c.exec)] = 1
-    return np.concatenate([ex, [np.log2(c.block), 1.0 if c.partition else 0.0,
-                                1.0 if (c.direct and c.exec != "atomic") else 0.0]]).astype(np.float32)
+    if c.exec == "atomic":
+        last = 0.0 if c.aggregate else 1.0
+    else:
+        last = 1.0 if c.direct else 0.0
+    return np.concatenate([ex, [np.log2(c.block), 1.0 if c.partition else 0.0, last]]).astype(np.float32)
 
 
 def features(mesh_f: np.ndarray, c: T.Candidate) -> np.ndarray:
@@ -174,7 +180,7 @@ def load_default() -> Optional[CostModel]:
 def corpus_candidates(loop: int) -> List[T.Candidate]:
     """Plan candidates of one (mesh, ordering): executors x block sizes x
     staging; partitioned variants are separate orderings."""
-    out = [T.Candidate(None, 0, "atomic", 256)]
+    out = [T.Candidate(None, 0, "atomic", 256), T.Candidate(None, 0, "atomic", 256, aggregate=False)]
     for b in (64, 128, 256, 512):
         out.append(T.Candidate(None, 0, "hier", b, False))
         out.append(T.Candidate(None, 0, "hier", b, True))
@@ -208,7 +214,12 @@ def mesh_for(loop: int, cells: float, seed: int) -> mg.MeshData:
 def generate(loops: Sequence[int], sizes: Sequence[float], seeds: Sequence[int],
              out_path: str = DEFAULT_CORPUS, iters_min_ms: float = 2.0, verbose: bool = True,
              time_limit_s: float = 1e9) -> dict:
-    """Time every (mesh, ordering, plan) and store features and log times."""
+    """Time every (mesh, ordering, plan) and store features and log times.
+
+    Per mesh group the info records the wall time of its exhaustive sweep
+    (orderings, plan builds and timings) and of its orderings alone: the
+    model's pick needs the orderings (its features are those of the ordered
+    mesh) but no plan build or timing, which is the tuning time it saves."""
     X, y, group, labels, secs_all = [], [], [], [], []
     info = []
     t_start = time.time()
@@ -218,22 +229,25 @@ def generate(loops: Sequence[int], sizes: Sequence[float], seeds: Sequence[int],
             for size in sizes:
                 if time.time() - t_start > time_limit_s:
                     break
+                t_group = time.time()
                 md = mesh_for(loop, size, seed)
                 cache = T.OrderedCache(md)
+                orders_s = 0.0
+                n0 = len(y)
                 for order, part in ORDERINGS:
                     t_o = time.time()
                     mdo = cache.get(order, part)
-                    order_s = time.time() - t_o
                     mf = mesh_features(mdo)
+                    orders_s += time.time() - t_o
                     for c in corpus_candidates(loop):
                         if part:
                             # blocks follow the parts: block size = part size
-                            blk = 256 if c.exec == "atomic" else part
                             if c.exec != "atomic" and c.block != 256:
                                 continue
-                            c = T.Candidate(order, part, c.exec, blk, c.direct)
+                            blk = 256 if c.exec == "atomic" else part
+                            c = T.Candidate(order, part, c.exec, blk, c.direct, c.aggregate)
                         else:
-                            c = T.Candidate(order, 0, c.exec, c.block, c.direct)
+                            c = T.Candidate(order, 0, c.exec, c.block, c.direct, c.aggregate)
                         try:
                             p, plan = T.build(mdo, c)
                             t1 = T.time_plan(p, plan, iters=2, warmup=1)
@@ -247,18 +261,43 @@ def generate(loops: Sequence[int], sizes: Sequence[float], seeds: Sequence[int],
                         secs_all.append(secs)
                         group.append(gid)
                         labels.append(c.label())
-                    if verbose:
-                        print(f"  {mg.LOOP_NAMES[loop]} {md.n_cells} seed {seed} {order}+{part}: "
-                              f"{len(y)} samples, order {order_s:.2f}s, total {time.time()-t_start:.0f}s",
-                              flush=True)
-                info.append({"gid": gid, "loop": loop, "cells": md.n_cells, "seed": seed})
+                sweep_s = time.time() - t_group
+                info.append({"gid": gid, "loop": int(loop), "cells": int(md.n_cells), "seed": int(seed),
+                             "size": float(size), "samples": len(y) - n0,
+                             "sweep_s": round(sweep_s, 3), "orders_s": round(orders_s, 3)})
+                if verbose:
+                    print(f"  {mg.LOOP_NAMES[loop]} {md.n_cells} seed {seed}: {len(y) - n0} samples, "
+                          f"sweep {sweep_s:.1f}s (orderings {orders_s:.1f}s), total {len(y)} samples, "
+                          f"{time.time()-t_start:.0f}s", flush=True)
                 gid += 1
                 del cache
     data = {"X": np.array(X, np.float32), "y": np.array(y, np.float32),
             "seconds": np.array(secs_all, np.float64), "group": np.array(group, np.int32),
             "label": np.array(labels), "info": json.dumps(info)}
     if out_path:
-        os.makedirs(os.path.dirname(out_path), exist_ok=True)
+        os.makedirs(os.path.dirname(os.path.abspath(out_path)), exist_ok=True)
+        np.savez_compressed(out_path, **data)
+    return data
+
+
+def merge(paths: Sequence[str], out_path: str = DEFAULT_CORPUS) -> dict:
+    """Concatenate corpus shards, renumbering their mesh groups."""
+    X, y, secs, group, labels, info = [], [], [], [], [], []
+    base = 0
+    for pth in paths:
+        d = load_corpus(pth)
+        inf = json.loads(str(d["info"]))
+        remap = {e["gid"]: base + i for i, e in enumerate(inf)}
+        for i, e in enumerate(inf):
+            e = dict(e)
+            e["gid"] = base + i
+            info.append(e)
+        X.append(d["X"]); y.append(d["y"]); secs.append(d["seconds"]); labels.append(d["label"])
+        group.append(np.array([remap[int(g)] for g in d["group"]], np.int32))
+        base += len(inf)
+    data = {"X": np.concatenate(X), "y": np.concatenate(y), "seconds": np.concatenate(secs),
+            "group": np.concatenate(group), "label": np.concatenate(labels), "info": json.dumps(info)}
+    if out_path:
         np.savez_compressed(out_path, **data)
     return data
 
@@ -306,3 +345,78 @@ def pick(model: CostModel, md: mg.MeshData, candidates: List[T.Candidate]) -> T.
         cands.append(c)
     pred = model.predict(np.array(rows))
     return cands[int(np.argmin(pred))]
+
+
+# ---------------------------------------------------------------------------
+# command line
+# ---------------------------------------------------------------------------
+DEFAULT_SIZES = (1e4, 4e4, 1.6e5, 6.4e5, 2.5e6, 1e7)
+
+
+def train_and_evaluate(data: dict, holdout_seed: Optional[int] = None, epochs: int = 200,
+                       seed: int = 1) -> tuple:
+    """Train on every seed but the held-out one (default: the largest) and
+    evaluate there: regret vs the sweep, the fixed default's regret, and the
+    tuning time the model saves on the held-out meshes."""
+    info = json.loads(str(data["info"]))
+    seed_of = {d["gid"]: d["seed"] for d in info}
+    seeds = np.array([seed_of[int(g)] for g in data["group"]])
+    hold = int(seeds.max()) if holdout_seed is None else int(holdout_seed)
+    train = seeds != hold
+    m = CostModel(seed=seed)
+    t0 = time.time()
+    losses = m.fit(data["X"][train], data["y"][train], epochs=epochs, batch=256, lr=2e-3)
+    train_s = time.time() - t0
+    ev = evaluate(m, data, ~train)
+    held = [d for d in info if d["seed"] == hold]
+    sweep_s = sum(d.get("sweep_s", 0.0) for d in held)
+    orders_s = sum(d.get("orders_s", 0.0) for d in held)
+    ev.update({"holdout_seed": hold, "train_rows": int(train.sum()), "test_rows": int((~train).sum()),
+               "final_loss": float(losses[-1]), "train_s": round(train_s, 2),
+               "heldout_sweep_s": round(sweep_s, 1), "heldout_orderings_s": round(orders_s, 1),
+               "tuning_time_saved_frac": (1.0 - orders_s / sweep_s) if sweep_s > 0 else None})
+    return m, ev
+
+
+def main(argv=None) -> int:
+    import argparse
+    ap = argparse.ArgumentParser(prog="python -m cuda_fot_b200.costmodel")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    g = sub.add_parser("generate", help="time (mesh, ordering, plan) triples on this GPU")
+    g.add_argument("--seeds", type=int, nargs="+", default=[1])
+    g.add_argument("--loops", nargs="+", default=list(mg.LOOP_NAMES))
+    g.add_argument("--sizes", type=float, nargs="+", default=list(DEFAULT_SIZES))
+    g.add_argument("--out", default=DEFAULT_CORPUS)
+    g.add_argument("--time-limit", type=float, default=1e9)
+    mg_ = sub.add_parser("merge", help="concatenate corpus shards")
+    mg_.add_argument("shards", nargs="+")
+    mg_.add_argument("--out", default=DEFAULT_CORPUS)
+    t = sub.add_parser("train", help="train on the corpus, evaluate on a held-out seed, save")
+    t.add_argument("--corpus", default=DEFAULT_CORPUS)
+    t.add_argument("--holdout-seed", type=int)
+    t.add_argument("--epochs", type=int, default=200)
+    t.add_argument("--out", default=DEFAULT_MODEL)
+    t.add_argument("--report")
+    a = ap.parse_args(argv)
+    if a.cmd == "generate":
+        loops = [mg.LOOP_NAMES.index(x) if not str(x).isdigit() else int(x) for x in a.loops]
+        d = generate(loops, a.sizes, a.seeds, a.out, time_limit_s=a.time_limit)
+        print(f"{len(d['y'])} samples -> {a.out}")
+    elif a.cmd == "merge":
+        d = merge(a.shards, a.out)
+        print(f"{len(d['y'])} samples, {len(json.loads(str(d['info'])))} mesh groups -> {a.out}")
+    else:
+        data = load_corpus(a.corpus)
+        m, ev = train_and_evaluate(data, a.holdout_seed, a.epochs)
+        m.save(a.out)
+        ev_short = {k: v for k, v in ev.items() if k != "picks"}
+        print(json.dumps(ev_short, indent=1))
+        if a.report:
+            with open(a.report, "w") as f:
+                json.dump(ev, f, indent=1)
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+    sys.exit(main())

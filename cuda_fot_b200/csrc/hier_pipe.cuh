@@ -5,11 +5,12 @@
 // claims (tiles = blocks in block-colour order, iteration after iteration):
 //   * the RECORD warp claims tiles from the plan's queue and copies each
 //     tile's record (header, point lists, local indices, per-point
-//     contribution lists, dependency list; built by plan.cu) into one of four
-//     record slots with a bulk copy on the TMA engine (no multicast).  Once
-//     the compute threads have written a tile back it refills the tile's slot
-//     with the tile four places ahead and publishes the tile's completion
-//     flag (per block: iterations completed, counted from Ctl::base);
+//     contribution lists, dependency list; built by plan.cu) into one of
+//     kRecSlots record slots with a bulk copy on the TMA engine (no
+//     multicast).  Once the compute threads have written a tile back it
+//     refills the tile's slot with the tile kRecSlots places ahead and
+//     publishes the tile's completion flag (per block: iterations completed,
+//     counted from Ctl::base);
 //   * the STAGING warp gathers a tile's read rows into one of two row slots
 //     with cp.async, then polls the completion flags of the blocks the tile
 //     conflicts with and, once they hold, prefetches the tile's output rows;
@@ -222,7 +223,7 @@ template <class L, int T> constexpr int ws_min_blocks() {
   return (65536 / ((T + 64) * L::kRegCap)) > 0 ? 65536 / ((T + 64) * L::kRegCap) : 1;
 }
 
-constexpr uint32_t kRecSlots = 4;
+constexpr uint32_t kRecSlots = 2;
 
 template <class L, bool SOA, int T>
 __global__ void __launch_bounds__(T + 64, ws_min_blocks<L, T>())
@@ -267,9 +268,9 @@ __global__ void __launch_bounds__(T + 64, ws_min_blocks<L, T>())
   if (warp == kRecordWarp) {
     // ---------------------------------------------------------------- record
     if (lane == 0) {
-      uint32_t uses[kRecSlots] = {0, 0, 0, 0};  // copies issued per slot
-      bool valid[kRecSlots] = {false, false, false, false};
-      uint32_t blk[kRecSlots] = {0, 0, 0, 0};
+      uint32_t uses[kRecSlots] = {};  // copies issued per slot
+      bool valid[kRecSlots] = {};
+      uint32_t blk[kRecSlots] = {};
       // claim pipeline: ticket t_a with its record offsets loaded, ticket t_b
       // claimed one refill earlier
       uint32_t t_a = atomicAdd(&P.ctl->ticket, 1u);

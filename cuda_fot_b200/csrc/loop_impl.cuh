@@ -111,11 +111,11 @@ void smem_layout(uint32_t cap0, uint32_t cap1, uint32_t variant, uint32_t rec_ca
   SmemLayout s;
   size_t off = 0;
   if (variant & kVariantPipe) {
-    // 4 tile-record slots, 2 read-row slots, the per-slot increments, 2
+    // kRecSlots tile-record slots, 2 read-row slots, the per-slot increments, 2
     // prefetched-output-row slots (AOS output rows of a multiple of 16 bytes)
     auto a128 = [](size_t v) { return (v + 127) & ~size_t(127); };
     s.rec_slot = (uint32_t)a128(rec_cap);
-    off = 4 * (size_t)s.rec_slot;
+    off = kRecSlots * (size_t)s.rec_slot;
     s.rows_off = (uint32_t)off;
     size_t rows = 0;
     for (int r = 0; r < L::kNumRead; ++r) {

@@ -23,7 +23,9 @@ import numpy as np
 from . import meshgen as mg
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libfot.so")
+# FOT_LIBRARY selects another build of the library (e.g. one compiled with
+# `python -m cuda_fot_b200.build --functor-dir DIR --out PATH`)
+LIB_PATH = os.environ.get("FOT_LIBRARY") or os.path.join(_HERE, "libfot.so")
 
 FOT_OK = 0
 AOS, SOA = 0, 1

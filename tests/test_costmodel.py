@@ -37,7 +37,7 @@ def test_features_shape_and_content():
     f = CM.features(mf, T.Candidate("gps", 0, "hier", 256, True))
     assert f.shape == (CM.N_FEATURES,) and np.all(np.isfinite(f))
     assert f[CM.FEATURES.index("loop_res_calc")] == 1
-    assert f[CM.FEATURES.index("exec_hier")] == 1 and f[CM.FEATURES.index("direct_reads")] == 1
+    assert f[CM.FEATURES.index("exec_hier")] == 1 and f[CM.FEATURES.index("direct_reads_or_plain_atomics")] == 1
     assert abs(f[CM.FEATURES.index("log2_block")] - 8) < 1e-6
 
 
@@ -93,15 +93,7 @@ def test_trained_model_regret_on_held_out_seeds():
     from cuda_fot_b200 import costmodel as CM
     if not os.path.exists(CM.DEFAULT_CORPUS):
         pytest.skip("no committed corpus")
-    import json
     data = CM.load_corpus()
-    info = json.loads(str(data["info"]))
-    seed_of = {d["gid"]: d["seed"] for d in info}
-    seeds = np.array([seed_of[g] for g in data["group"]])
-    test_seed = seeds.max()
-    train = seeds != test_seed
-    m = CM.CostModel(seed=1)
-    m.fit(data["X"][train], data["y"][train], epochs=200, batch=256, lr=2e-3)
-    ev = CM.evaluate(m, data, ~train)
+    _, ev = CM.train_and_evaluate(data)
     assert ev["mean_regret"] <= 0.05, ev
     assert ev["default_mean_regret"] is None or ev["mean_regret"] < ev["default_mean_regret"], ev
