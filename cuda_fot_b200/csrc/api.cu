@@ -545,6 +545,20 @@ int fot_sync(fot_problem *p, void *stream) {
   return FOT_OK;
 }
 
+int fot_plan_inject_lost_flag(fot_plan *plan, uint32_t block) {
+  if (!plan) return fail(FOT_ERR_ARG, "null plan");
+  if (!(plan->variant & kVariantPipe) || !plan->block_done.ptr)
+    return fail(FOT_ERR_STATE, "the plan does not run the pipelined hierarchical kernel");
+  if (block >= plan->n_blocks) return fail(FOT_ERR_ARG, "block %u out of range (%u blocks)", block, plan->n_blocks);
+  FOT_CUDA(cudaDeviceSynchronize());
+  Ctl c{};
+  FOT_CUDA(cudaMemcpy(&c, plan->ctl.ptr, sizeof(Ctl), cudaMemcpyDeviceToHost));
+  if (c.base == 0) return fail(FOT_ERR_STATE, "run the plan at least once before injecting");
+  FOT_CUDA(cudaMemset(plan->block_done.as<unsigned int>() + block, 0, sizeof(unsigned int)));
+  FOT_CUDA(cudaDeviceSynchronize());
+  return FOT_OK;
+}
+
 int fot_graph_create(fot_problem *p, fot_plan *plan, uint32_t iterations, void *stream,
                      fot_graph **out) {
   if (!p || !plan || !out) return fail(FOT_ERR_ARG, "null argument");

@@ -149,6 +149,11 @@ class Plan:
     def graph(self, iterations: int, stream=None) -> "Graph":
         return Graph(self, iterations, stream)
 
+    def inject_lost_flag(self, block: int) -> None:
+        """Test hook (fot_plan_inject_lost_flag): lose one block's completion
+        flag so that the next run's dependency waits hit their time limit."""
+        _check(_lib.fot_plan_inject_lost_flag(self._h, C.c_uint32(block)))
+
     def __del__(self):
         if getattr(self, "_h", None) is not None and self._h.value:
             _lib.fot_plan_destroy(self._h)
@@ -170,6 +175,30 @@ class Graph:
     def __del__(self):
         if getattr(self, "_h", None) is not None and self._h.value:
             _lib.fot_graph_destroy(self._h)
+            self._h = None
+
+
+class Batch:
+    """Hierarchical plans of many problems run by ONE persistent launch over a
+    (mesh, block colour) tile queue (fot_batch)."""
+
+    def __init__(self, plans: List[Plan]):
+        self.plans = list(plans)  # keeps the problems and plans alive
+        n = len(self.plans)
+        probs = (C.c_void_p * n)(*[pl.problem._h.value for pl in self.plans])
+        hs = (C.c_void_p * n)(*[pl._h.value for pl in self.plans])
+        self._h = C.c_void_p()
+        _check(_lib.fot_batch_create(probs, hs, C.c_uint32(n), C.byref(self._h)))
+
+    def run(self, iterations: int = 1, stream=None) -> None:
+        _check(_lib.fot_batch_run(self._h, C.c_uint32(iterations), _stream_ptr(stream)))
+
+    def sync(self, stream=None) -> None:
+        _check(_lib.fot_batch_sync(self._h, _stream_ptr(stream)))
+
+    def __del__(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.fot_batch_destroy(self._h)
             self._h = None
 
 

@@ -227,6 +227,16 @@ int fot_run(fot_problem *p, fot_plan *plan, uint32_t iterations, void *stream);
 /* Wait for the problem's work on `stream` and report device-side errors. */
 int fot_sync(fot_problem *p, void *stream);
 
+/* Fault injection for tests of the failure path (no counterpart in the
+ * reference).  Zeroes the completion flag of `block` (plan order) of a
+ * pipelined hierarchical plan that has run at least once, as if the block's
+ * last completion had been lost.  In the next fot_run the tiles that depend
+ * on the block wait for it until their time limit (about 2 s), the kernel
+ * returns early, and fot_sync reports FOT_ERR_DEVICE and resets the plan's
+ * queue and flags: the problem's data are then undefined, the plan and the
+ * CUDA context stay usable.  Synchronous. */
+int fot_plan_inject_lost_flag(fot_plan *plan, uint32_t block);
+
 /* Capture `iterations` iterations of fot_run into a CUDA graph and replay it. */
 int fot_graph_create(fot_problem *p, fot_plan *plan, uint32_t iterations,
                      void *stream, fot_graph **out);
