@@ -90,7 +90,12 @@ template <class L, bool SOA> struct GlobalRows {
   uint32_t p[2][L::kDim];
   template <int R> __device__ __forceinline__ const T *ptr(int s) const {
     const uint32_t q = p[L::read_class(R)][s];
-    return base[R] + (SOA ? (size_t)q : (size_t)q * L::read_dim(R));
+    const T *r = base[R] + (SOA ? (size_t)q : (size_t)q * L::read_dim(R));
+    // AOS rows of a multiple of 16 bytes start 16-byte aligned: the compiler
+    // may then merge neighbouring element loads into vector loads
+    if constexpr (!SOA && (L::read_dim(R) * sizeof(T)) % 16 == 0)
+      return static_cast<const T *>(__builtin_assume_aligned(r, 16));
+    return r;
   }
   template <int R> __device__ __forceinline__ unsigned stride() const {
     return SOA ? np[R] : 1u;
@@ -103,7 +108,10 @@ template <class L> struct SmemRows {
   const T *base[L::kNumRead > 0 ? L::kNumRead : 1];
   uint16_t l[2][L::kDim];
   template <int R> __device__ __forceinline__ const T *ptr(int s) const {
-    return base[R] + (uint32_t)l[L::read_class(R)][s] * L::read_dim(R);
+    const T *r = base[R] + (uint32_t)l[L::read_class(R)][s] * L::read_dim(R);
+    if constexpr ((L::read_dim(R) * sizeof(T)) % 16 == 0)
+      return static_cast<const T *>(__builtin_assume_aligned(r, 16));
+    return r;
   }
   template <int R> __device__ __forceinline__ unsigned stride() const { return 1u; }
 };

@@ -19,8 +19,10 @@
 //     thread-colour order -- the order of the reference's colour-by-colour
 //     shared accumulation, so results stay bit-identical to the CPU replay --
 //     and store out[p] + sum.
-// The roles hand over through mbarriers (record landed, rows landed, output
-// rows landed / dependencies held, tile written back); the compute threads
+// The roles hand over through mbarriers (record landed, rows landed, rows
+// consumed, output rows landed / dependencies held, tile written back): a
+// row slot is refilled as soon as the compute phase that read it ends, so the
+// next-but-one tile's rows load during a tile's write-back; the compute threads
 // also meet at a named barrier three times per tile.  The claim, the record
 // copy and the flag release therefore stay off the compute threads' path.
 // Every wait is bounded: after about two seconds the kernel sets
@@ -218,15 +220,11 @@ __device__ __forceinline__ void ws_stage_rows(const LoopData &d, const HierPlanD
   });
 }
 
-// Resident CTAs per SM the kernel's register cap aims for (T + 64 threads).
-template <class L, int T> constexpr int ws_min_blocks() {
-  return (65536 / ((T + 64) * L::kRegCap)) > 0 ? 65536 / ((T + 64) * L::kRegCap) : 1;
-}
-
-constexpr uint32_t kRecSlots = 2;
+constexpr uint32_t kRecSlots = 3;
 
 template <class L, bool SOA, int T>
-__global__ void __launch_bounds__(T + 64, ws_min_blocks<L, T>())
+// registers capped at the loop's kRegCap for every thread of the CTA
+__global__ void __launch_bounds__(T + 64) __maxnreg__(L::kRegCap)
     k_hier_pipe(LoopData d, HierPlanDev P) {
   using out_t = typename L::out_t;
   using read_t = typename L::read_t;
@@ -239,6 +237,7 @@ __global__ void __launch_bounds__(T + 64, ws_min_blocks<L, T>())
   __shared__ __align__(8) uint64_t s_tile_done[kRecSlots];
   __shared__ __align__(8) uint64_t s_rows_full[2];
   __shared__ __align__(8) uint64_t s_out_full[2];
+  __shared__ __align__(8) uint64_t s_rows_empty[2];
   __shared__ uint32_t s_iter[kRecSlots];   // iteration of the tile in each record slot
   __shared__ uint32_t s_valid[kRecSlots];  // 0: no tile (end of this CTA's queue)
   __shared__ uint32_t s_abort[2];          // per row slot: skip the write-back
@@ -257,6 +256,7 @@ __global__ void __launch_bounds__(T + 64, ws_min_blocks<L, T>())
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&s_rows_full[b], 33);
+      mbar_init(&s_rows_empty[b], 1);
       mbar_init(&s_out_full[b], 33);
     }
     mbar_fence_init();
@@ -336,9 +336,8 @@ __global__ void __launch_bounds__(T + 64, ws_min_blocks<L, T>())
     for (uint32_t j = 0;; ++j) {
       const uint32_t s = j % kRecSlots, b = j & 1u;
       bool ok = mbar_wait_or_stop(&s_rec_full[s], (j / kRecSlots) & 1u, &s_stop);
-      // the row slot and output slot of tile j - 2 are free once it is written back
-      if (ok && j >= 2)
-        ok = mbar_wait_or_stop(&s_tile_done[(j - 2) % kRecSlots], ((j - 2) / kRecSlots) & 1u, &s_stop);
+      // the row slot of tile j - 2 is free once that tile's compute phase ended
+      if (ok && j >= 2) ok = mbar_wait_or_stop(&s_rows_empty[b], ((j - 2) >> 1) & 1u, &s_stop);
       ok = __all_sync(0xFFFFFFFFu, ok);
       if (!ok || err || !s_valid[s]) {
         if (!ok && !err) {
@@ -357,9 +356,13 @@ __global__ void __launch_bounds__(T + 64, ws_min_blocks<L, T>())
       ws_stage_rows<L, SOA>(d, P, rows_base + b * P.rows_bytes, m);
       mbar_arrive_cp_async(&s_rows_full[b]);
       if (lane == 0) mbar_arrive(&s_rows_full[b]);
-      // dependencies, then the output rows
-      const bool dep_ok = wait_deps(m, base + s_iter[s], P.block_done, &s_stop);
+      // dependencies, then the output rows (into the output slot of tile
+      // j - 2, free once that tile is written back)
+      bool dep_ok = wait_deps(m, base + s_iter[s], P.block_done, &s_stop);
       fence_acq_rel_gpu();
+      if (dep_ok && j >= 2)
+        dep_ok = __all_sync(0xFFFFFFFFu, mbar_wait_or_stop(&s_tile_done[(j - 2) % kRecSlots],
+                                                           ((j - 2) / kRecSlots) & 1u, &s_stop));
       if (kPrefetchOut && dep_ok) {
         constexpr int CH = ROW_OUT / 16;
         char *ob = reinterpret_cast<char *>(smem + P.outbuf_off + b * P.outbuf_bytes);
@@ -415,6 +418,7 @@ __global__ void __launch_bounds__(T + 64, ws_min_blocks<L, T>())
           for (int k = 0; k < K; ++k) inc[(k * D + q) * T + tid] = v[q][k];
       }
       named_bar_sync<T>();
+      if (tid == 0) mbar_arrive(&s_rows_empty[b]);  // the row slot may be refilled
       const bool ok_out = mbar_wait_or_stop(&s_out_full[b], ph, &s_stop);
       if (ok_out && !s_abort[b]) {
         const out_t *ob = reinterpret_cast<const out_t *>(smem + P.outbuf_off + b * P.outbuf_bytes);
