@@ -27,6 +27,7 @@ from . import meshgen as mg
 from . import tune as T
 
 N_FEATURES = 24
+NOALLOC_MAX_ROWS = 4096  # FOT_MODEL_NOALLOC_MAX_ROWS
 HERE = os.path.dirname(os.path.abspath(__file__))
 MODEL_DIR = os.path.join(HERE, "model")
 DEFAULT_MODEL = os.path.join(MODEL_DIR, "costmodel.npz")
@@ -127,6 +128,15 @@ class CostModel:
         X = np.ascontiguousarray(X, np.float32)
         y = np.zeros(X.shape[0], np.float32)
         F._check(_lib.fot_model_predict(self._h, X.ctypes.data_as(_fp), X.shape[0], y.ctypes.data_as(_fp)))
+        return y
+
+    def predict_noalloc(self, X: np.ndarray) -> np.ndarray:
+        """predict() through fot_model_predict_noalloc: no device allocation
+        per call, at most NOALLOC_MAX_ROWS rows, calls must not overlap."""
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.zeros(X.shape[0], np.float32)
+        F._check(_lib.fot_model_predict_noalloc(self._h, X.ctypes.data_as(_fp), X.shape[0],
+                                                y.ctypes.data_as(_fp)))
         return y
 
     def grad(self, X: np.ndarray, t: np.ndarray):

@@ -278,6 +278,48 @@ int fot_model_predict(fot_model *M, const float *X, int n, float *y) {
   return FOT_OK;
 }
 
+} // extern "C"
+
+namespace {
+// Device scratch of fot_model_predict_noalloc: rows x IN inputs, then rows
+// outputs.  Nothing in it has to start at zero: a call copies its inputs in
+// and the forward kernel writes every output row it copies back.
+constexpr int kNoAllocRows = FOT_MODEL_NOALLOC_MAX_ROWS;
+static __device__ __align__(256) float g_noalloc_scratch[(size_t)kNoAllocRows * (IN + 1)];
+constexpr int kMaxDevices = 64;
+float *g_noalloc_ptr[kMaxDevices] = {};  // per device, set by its first call
+} // namespace
+
+extern "C" {
+
+int fot_model_predict_noalloc(fot_model *M, const float *X, int n, float *y) {
+  if (!M || !X || !y || n <= 0) return fail(FOT_ERR_ARG, "bad argument");
+  if (n > kNoAllocRows)
+    return fail(FOT_ERR_LIMIT,
+                "fot_model_predict_noalloc takes at most %d rows per call (got %d): split the "
+                "rows over several calls or use fot_model_predict",
+                kNoAllocRows, n);
+  int dev = 0;
+  FOT_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return fail(FOT_ERR_LIMIT, "device %d out of range", dev);
+  if (!g_noalloc_ptr[dev]) {  // setup, once per device
+    void *p = nullptr;
+    FOT_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    FOT_CUDA(cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(NPARAM * sizeof(float))));
+    g_noalloc_ptr[dev] = static_cast<float *>(p);
+  }
+  float *dX = g_noalloc_ptr[dev];
+  float *dy = dX + (size_t)kNoAllocRows * IN;
+  FOT_CUDA(cudaMemcpy(dX, X, (size_t)n * IN * 4, cudaMemcpyHostToDevice));
+  k_forward<<<(n + TPB - 1) / TPB, TPB, NPARAM * sizeof(float)>>>(
+      M->params.as<float>(), M->mean.as<float>(), M->inv_std.as<float>(), dX, nullptr, n, 0.f, dy,
+      Acts{});
+  FOT_CUDA(cudaGetLastError());
+  FOT_CUDA(cudaMemcpy(y, dy, (size_t)n * 4, cudaMemcpyDeviceToHost));
+  return FOT_OK;
+}
+
 int fot_model_grad(fot_model *M, const float *X, const float *t, int n, float *grad, float *loss) {
   if (!M || !X || !t || n <= 0) return fail(FOT_ERR_ARG, "bad argument");
   Batch B;

@@ -273,6 +273,21 @@ int fot_model_get_params(const fot_model *m, float *params);
 int fot_model_set_normalisation(fot_model *m, const float *mean, const float *stddev);
 /* y[i] = model(X[i]) for n feature rows X (n x FOT_MODEL_FEATURES) */
 int fot_model_predict(fot_model *m, const float *X, int n, float *y);
+
+/* fot_model_predict without any device allocation (no counterpart in the
+ * reference).  For callers that must not allocate device memory once they
+ * are running: the inputs and outputs of the call are staged in a fixed
+ * file-scope device array of FOT_MODEL_NOALLOC_MAX_ROWS rows (25 floats per
+ * row, 409,600 bytes) instead of buffers allocated per call.  More rows
+ * than that: FOT_ERR_LIMIT, nothing is computed.  No part of the array has
+ * to start at zero (a call writes every row it reads).  All calls on one
+ * device share the array, so calls that overlap in time (from several host
+ * threads) race and must be serialised by the caller.  The first call on a
+ * device does the setup (looks up the array's address, sets the kernel's
+ * shared-memory limit) and should come before any stream capture.  Same
+ * results as fot_model_predict.  Synchronous. */
+#define FOT_MODEL_NOALLOC_MAX_ROWS 4096
+int fot_model_predict_noalloc(fot_model *m, const float *X, int n, float *y);
 /* gradient of 0.5/n * sum (model(X) - t)^2 w.r.t. the parameters, and the loss */
 int fot_model_grad(fot_model *m, const float *X, const float *t, int n, float *grad, float *loss);
 /* `epochs` passes of Adam over contiguous minibatches of `batch` rows;
