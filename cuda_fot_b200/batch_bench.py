@@ -5,11 +5,12 @@
 Workload: `--meshes` meshes, half res_calc 2D quad meshes (edge -> cell
 increment, FP64) and half volna shallow-water triangle meshes (edge flux
 added to 2 cells, FP32), with cell counts drawn log-uniform between 4,000 and
-1,000,000 from the seed.  Every mesh gets a hierarchical plan; the block size
-of the batch is chosen by the autotuner (measured, 64 / 128 / 256), then:
+1,000,000 from the seed.  The autotuner measures the batch under each plan
+kind (atomic with / without warp aggregation, hierarchical with blocks of 64,
+128, 256) and keeps the fastest, then:
 
-  * batch_graph: a CUDA graph of `--timesteps` batched launches (one
-    persistent launch per timestep over all meshes' tiles), replayed;
+  * batch_graph: a CUDA graph of `--timesteps` batched launches (one launch
+    per timestep over all meshes' tiles), replayed;
   * batch_run:   the same timesteps as one Plan-like call (one launch);
   * loop_atomic: the plain method, one atomic launch per mesh per timestep
     from the host (`--meshes` x `--timesteps` launches);
@@ -73,30 +74,37 @@ def main(argv=None) -> int:
     ub = float(sum(md.unique_bytes() for md in mds))
     n_cells = {"res_calc": int(sum(md.n_points[0] for md in mds if md.loop == mg.RES_CALC)),
                "volna": int(sum(md.n_points[0] for md in mds if md.loop == mg.VOLNA))}
+    # two copies of every mesh on the GPU: hierarchical plans renumber their
+    # problem's cells into colour order, atomic plans run on the given order
     t0 = time.time()
-    probs = [F.Problem.from_mesh(md) for md in mds]
+    probs_a = [F.Problem.from_mesh(md) for md in mds]
+    probs_h = [F.Problem.from_mesh(md) for md in mds]
     upload_s = time.time() - t0
     st = torch.cuda.Stream()
     T = a.timesteps
 
-    # autotuned block size of the batch (hierarchical plans of every mesh)
+    # the autotuner's choice of the batch's plan kind and block size
+    kinds = [("atomic", F.EXEC_ATOMIC, 256, 0), ("atomic-plain", F.EXEC_ATOMIC, 256, F.PLAN_NO_AGGREGATE),
+             ("hier/64", F.EXEC_HIER, 64, 0), ("hier/128", F.EXEC_HIER, 128, 0),
+             ("hier/256", F.EXEC_HIER, 256, 0)]
     tune = {}
     best = None
-    for blk in (64, 128, 256):
+    for name, ex, blk, flags in kinds:
         t1 = time.time()
-        plans = [p.plan(F.EXEC_HIER, blk) for p in probs]
+        probs = probs_a if ex == F.EXEC_ATOMIC else probs_h
+        plans = [p.plan(ex, blk, flags) for p in probs]
         plan_s = time.time() - t1
         b = F.Batch(plans)
         b.run(2, st)
         b.sync(st)
         secs = timed(lambda: b.run(5, st), st) / 5
         b.sync(st)
-        tune[blk] = {"us_per_step": secs * 1e6, "gbs": ub / secs / 1e9, "plan_build_s": round(plan_s, 2)}
+        tune[name] = {"us_per_step": secs * 1e6, "gbs": ub / secs / 1e9, "plan_build_s": round(plan_s, 2)}
         if best is None or secs < best[1]:
-            best = (blk, secs)
+            best = ((name, ex, blk, flags), secs)
         del b, plans
-    blk = best[0]
-    plans = [p.plan(F.EXEC_HIER, blk) for p in probs]
+    name, ex, blk, flags = best[0]
+    plans = [p.plan(ex, blk, flags) for p in (probs_a if ex == F.EXEC_ATOMIC else probs_h)]
     batch = F.Batch(plans)
     batch.run(2, st)
     batch.sync(st)
@@ -117,18 +125,21 @@ def main(argv=None) -> int:
     secs = timed(lambda: batch.run(T, st), st) / T
     batch.sync(st)
     res["batch_run"] = secs
+    del batch, plans
     # per-mesh hierarchical launches from the host
+    hplans = [p.plan(F.EXEC_HIER, 128) for p in probs_h]
+
     def loop_hier():
-        for pl in plans:
+        for pl in hplans:
             pl.run(1, st)
     loop_hier()
     torch.cuda.synchronize()
-    res["loop_hier"] = timed(loop_hier, st, min(T, 10))
-    for p in probs:
+    res["loop_hier"] = timed(loop_hier, st, 3)
+    for p in probs_h:
         p.sync(st)
-    del batch, plans
+    del hplans
     # the plain method: one atomic launch per mesh per timestep
-    aplans = [p.plan(F.EXEC_ATOMIC, 256, F.PLAN_NO_AGGREGATE) for p in probs]
+    aplans = [p.plan(F.EXEC_ATOMIC, 256, F.PLAN_NO_AGGREGATE) for p in probs_a]
 
     def loop_atomic():
         for pl in aplans:
@@ -144,13 +155,13 @@ def main(argv=None) -> int:
     torch.cuda.synchronize()
     res["loop_atomic_graph"] = timed(g2.replay, torch.cuda.current_stream(), 3) / min(T, 10)
     del g2
-    for p in probs:
+    for p in probs_a:
         p.sync(st)
 
     line = {"metric": "batched indirect loops, aggregate GB/s of unique bytes",
             "unit": "GB/s", "meshes": a.meshes, "timesteps": T, "seed": a.seed,
             "cells": n_cells, "unique_bytes_per_step": ub,
-            "block_size": blk, "autotune": tune,
+            "batch_plan": name, "autotune": tune,
             "us_per_step": {k: v * 1e6 for k, v in res.items()},
             "gbs": {k: ub / v / 1e9 for k, v in res.items()},
             "speedup_batch_graph_vs_loop_atomic": res["loop_atomic"] / res["batch_graph"],

@@ -384,6 +384,22 @@ int fot_plan_build(fot_problem *p, const fot_plan_desc *desc, fot_plan **out) {
       plan->threads = hier_threads(desc->block_size);
       ops->smem_layout(plan->cap[0], plan->cap[1], plan->variant, plan->rec_cap, plan->threads,
                        &plan->layout);
+      // a third tile-record slot deepens the pipelined kernel's look-ahead;
+      // keep it only when it costs no resident CTA
+      if ((plan->variant & kVariantPipe) && plan->layout.total <= 227 * 1024) {
+        SmemLayout l3;
+        const uint32_t v3 = plan->variant | kVariantSlots3;
+        ops->smem_layout(plan->cap[0], plan->cap[1], v3, plan->rec_cap, plan->threads, &l3);
+        int per2 = 0, per3 = 0;
+        const bool soa = p->layout == FOT_SOA;
+        rc = ops->occupancy(desc->exec, soa, plan->threads, plan->variant, plan->layout.total, &per2);
+        if (rc == FOT_OK && l3.total <= 227 * 1024)
+          rc = ops->occupancy(desc->exec, soa, plan->threads, v3, l3.total, &per3);
+        if (rc == FOT_OK && per3 >= per2 && per3 > 0) {
+          plan->variant = v3;
+          plan->layout = l3;
+        }
+      }
       // the pipelined kernel holds two tiles' rows; when they do not fit,
       // the single-buffer persistent kernel runs the plan instead
       if ((plan->variant & kVariantPipe) && plan->layout.total > 227 * 1024) {

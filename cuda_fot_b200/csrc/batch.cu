@@ -1,9 +1,13 @@
-// Batched persistent executor: many meshes (problems with hierarchical
-// plans) in ONE launch.  CTAs claim tiles from one queue ordered by
-// (iteration, block colour, mesh, block); a tile waits only for its own
-// mesh's earlier colours, on a per-mesh counter, so meshes of very different
-// sizes share the GPU without a launch per mesh and colour.  The reference
-// has no counterpart (one mesh per process, one launch per colour).
+// Batched executors: many meshes in ONE launch.
+//   * hierarchical plans: CTAs claim tiles from one queue ordered by
+//     (iteration, block colour, mesh, block); a tile waits only for its own
+//     mesh's earlier colours, on a per-mesh counter, so meshes of very
+//     different sizes share the GPU without a launch per mesh and colour;
+//   * atomic plans: tiles of 1,024 consecutive cells of one mesh, for every
+//     mesh and every iteration, in one grid-stride launch (iterations need no
+//     ordering: the loops never read the dataset they increment).
+// The reference has no counterpart (one mesh per process, one launch per
+// colour).
 #define FOT_ADAPTER_ALL 1
 #include <algorithm>
 #include <numeric>
@@ -40,7 +44,7 @@ __device__ __forceinline__ void batch_tile(const BatchMesh &m, unsigned char *sm
 
 template <bool SOA, int T, class... Ls>
 __global__ void __launch_bounds__(T) k_batch(BatchDev B) {
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint32_t s_ticket;
   const uint32_t tid = threadIdx.x;
   for (;;) {
@@ -72,6 +76,54 @@ __global__ void __launch_bounds__(T) k_batch(BatchDev B) {
       __threadfence();
     }
   }
+}
+
+constexpr uint32_t kAtomicTile = 1024;  // cells per tile of the atomic batch
+
+template <class... Ls> constexpr int max_reg_cap() {
+  int m = 0;
+  ((m = Ls::kRegCap > m ? Ls::kRegCap : m), ...);
+  return m;
+}
+
+template <bool SOA, bool AGG, class... Ls>
+__global__ void __launch_bounds__(256, (65536 / (256 * max_reg_cap<Ls...>())) > 0
+                                           ? 65536 / (256 * max_reg_cap<Ls...>()) : 1)
+    k_batch_atomic(BatchDev B) {
+  const uint32_t warp = threadIdx.x >> 5;
+  for (uint32_t t = blockIdx.x; t < B.total_tiles; t += gridDim.x) {
+    const uint32_t r = t % B.tiles_per_iter;
+    const BatchMesh &m = B.mesh[B.tile_mesh[r]];
+    const uint32_t start = B.tile_block[r];
+#pragma unroll 1
+    for (uint32_t k = 0; k < kAtomicTile / 256; ++k) {
+      const uint32_t base = start + (k * 8u + warp) * 32u;
+      ((m.loop == Ls::kLoop ? (atomic_warp<Ls, SOA, AGG>(m.d, base), 0) : 0), ...);
+    }
+  }
+}
+
+template <bool SOA, bool AGG> const void *batch_atomic_kernel(uint32_t loop_mask) {
+  using RC = res_calc::Loop;
+  using MA = mini_aero::Loop;
+  using LU = lulesh::Loop;
+  using VO = volna::Loop;
+  using GA = getacc::Loop;
+  switch (loop_mask) {
+  case 1u << FOT_LOOP_RES_CALC: return (const void *)&k_batch_atomic<SOA, AGG, RC>;
+  case 1u << FOT_LOOP_MINI_AERO: return (const void *)&k_batch_atomic<SOA, AGG, MA>;
+  case 1u << FOT_LOOP_LULESH: return (const void *)&k_batch_atomic<SOA, AGG, LU>;
+  case 1u << FOT_LOOP_VOLNA: return (const void *)&k_batch_atomic<SOA, AGG, VO>;
+  case 1u << FOT_LOOP_GETACC: return (const void *)&k_batch_atomic<SOA, AGG, GA>;
+  case (1u << FOT_LOOP_RES_CALC) | (1u << FOT_LOOP_VOLNA):
+    return (const void *)&k_batch_atomic<SOA, AGG, RC, VO>;
+  }
+  return nullptr;
+}
+
+const void *batch_atomic_kernel_for(bool soa, bool agg, uint32_t loop_mask) {
+  if (soa) return agg ? batch_atomic_kernel<true, true>(loop_mask) : batch_atomic_kernel<true, false>(loop_mask);
+  return agg ? batch_atomic_kernel<false, true>(loop_mask) : batch_atomic_kernel<false, false>(loop_mask);
 }
 
 // Kernel variants: one loop kind, or the res_calc + volna pair.
@@ -123,6 +175,7 @@ struct fot_batch {
   size_t smem = 0;
   int per_sm = 0;
   bool soa = false;
+  bool atomic = false;  // atomic plans (else hierarchical)
   const void *kernel = nullptr;
 };
 
@@ -136,19 +189,32 @@ int fot_batch_create(fot_problem *const *problems, fot_plan *const *plans, uint3
   std::vector<BatchMesh> meshes(n);
   uint32_t mask = 0;
   int rc = FOT_OK;
+  B->atomic = plans[0] && plans[0]->desc.exec == FOT_EXEC_ATOMIC;
+  const bool agg = plans[0] && !(plans[0]->desc.flags & FOT_PLAN_NO_AGGREGATE);
   for (uint32_t i = 0; i < n && rc == FOT_OK; ++i) {
     fot_problem *p = problems[i];
     fot_plan *pl = plans[i];
     if (!p || !pl || pl->prob != p) rc = fail(FOT_ERR_ARG, "batch entry %u: plan/problem mismatch", i);
-    else if (pl->desc.exec == FOT_EXEC_ATOMIC) rc = fail(FOT_ERR_ARG, "batch entry %u is not hierarchical", i);
-    else if (pl->version != p->version) rc = fail(FOT_ERR_STATE, "batch entry %u: stale plan", i);
+    else if ((pl->desc.exec == FOT_EXEC_ATOMIC) != B->atomic)
+      rc = fail(FOT_ERR_ARG, "batch entry %u: a batch holds atomic plans only or hierarchical plans only", i);
+    else if (B->atomic && agg != !(pl->desc.flags & FOT_PLAN_NO_AGGREGATE))
+      rc = fail(FOT_ERR_ARG, "batch entry %u: atomic plans of a batch all aggregate or none does", i);
+    else if (!B->atomic && pl->version != p->version)
+      rc = fail(FOT_ERR_STATE, "batch entry %u: stale plan", i);
     else if (i > 0 && (p->layout == FOT_SOA) != B->soa) rc = fail(FOT_ERR_ARG, "batch mixes layouts");
     if (rc != FOT_OK) break;
     B->soa = p->layout == FOT_SOA;
     mask |= 1u << p->loop;
     meshes[i].d = p->loop_data();
-    meshes[i].P = pl->dev(1);
     meshes[i].loop = p->loop;
+    B->probs.push_back(p);
+    B->plans.push_back(pl);
+    B->versions.push_back(p->version);
+    if (B->atomic) {
+      B->threads = 256;
+      continue;
+    }
+    meshes[i].P = pl->dev(1);
     // the batched tiles use the staged one-tile-at-a-time layout
     SmemLayout lay;
     loop_ops(p->loop)->smem_layout(pl->cap[0], pl->cap[1], kVariantStage, 0, pl->threads, &lay);
@@ -157,22 +223,29 @@ int fot_batch_create(fot_problem *const *problems, fot_plan *const *plans, uint3
     meshes[i].P.pts_smem_off = lay.pts_off;
     B->threads = std::max(B->threads, pl->threads);
     B->smem = std::max(B->smem, lay.total);
-    B->probs.push_back(p);
-    B->plans.push_back(pl);
-    B->versions.push_back(p->version);
   }
   if (rc == FOT_OK && B->threads > 512)
     rc = fail(FOT_ERR_ARG, "batched plans must use block sizes of at most 512");
   if (rc == FOT_OK) {
-    B->kernel = batch_kernel_for(B->soa, B->threads, mask);
+    B->kernel = B->atomic ? batch_atomic_kernel_for(B->soa, agg, mask)
+                          : batch_kernel_for(B->soa, B->threads, mask);
     if (!B->kernel)
       rc = fail(FOT_ERR_ARG, "a batch holds one loop kind, or res_calc with volna");
   }
   if (rc == FOT_OK) {
-    // tile order: colour-major across meshes, then mesh, then block
+    // tile order: colour-major across meshes, then mesh, then block (atomic
+    // plans: mesh after mesh, kAtomicTile cells per tile)
     uint32_t max_col = 0;
     for (auto *pl : B->plans) max_col = std::max(max_col, pl->n_colours);
     std::vector<uint32_t> tm, tb;
+    if (B->atomic) {
+      for (uint32_t i = 0; i < n; ++i)
+        for (uint32_t c0 = 0; c0 < B->probs[i]->n_cells; c0 += kAtomicTile) {
+          tm.push_back(i);
+          tb.push_back(c0);
+        }
+      max_col = 0;
+    }
     for (uint32_t c = 0; c < max_col; ++c)
       for (uint32_t i = 0; i < n; ++i) {
         const fot_plan *pl = B->plans[i];
@@ -212,7 +285,10 @@ int fot_batch_run(fot_batch *B, uint32_t iterations, void *stream) {
   if (!B) return fail(FOT_ERR_ARG, "null batch");
   if (iterations == 0) return FOT_OK;
   for (size_t i = 0; i < B->probs.size(); ++i)
-    if (B->probs[i]->version != B->versions[i] || B->plans[i]->version != B->versions[i])
+    // the batch holds device views of each problem's data (and of each
+    // hierarchical plan): a reorder after creation invalidates them
+    if (B->probs[i]->version != B->versions[i] ||
+        (!B->atomic && B->plans[i]->version != B->versions[i]))
       return fail(FOT_ERR_STATE, "batch entry %zu changed since the batch was created", i);
   const uint64_t total = (uint64_t)iterations * B->tiles_per_iter;
   const uint32_t grid_max = (uint32_t)(B->per_sm * device_sm_count());

@@ -29,8 +29,9 @@ struct SmemLayout {
 // in shared memory (else gather them straight from HBM/L2); bit 1 = the
 // pipelined persistent kernel (warp-specialised: tile records by bulk copy,
 // double-buffered staging, per-point gather of the increments), launched
-// with 64 threads more than `threads` for its two control warps.
-constexpr uint32_t kVariantStage = 1u, kVariantPipe = 2u;
+// with 64 threads more than `threads` for its two control warps; bit 2 = that
+// kernel with three tile-record slots (else two).
+constexpr uint32_t kVariantStage = 1u, kVariantPipe = 2u, kVariantSlots3 = 4u;
 
 struct LoopOps {
   // launch one iteration of the atomic executor

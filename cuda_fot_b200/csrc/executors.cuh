@@ -157,72 +157,79 @@ __device__ __forceinline__ void load_row(const uint32_t *__restrict__ map, uint3
 
 template <class T> __device__ __forceinline__ void atomic_add(T *a, T v) { atomicAdd(a, v); }
 
+// Cells [base, base + 32) of one mesh, one per lane of the calling warp
+// (cells past n_cells are masked): compute, optionally aggregate by target
+// point, add with atomics.
 template <class L, bool SOA, bool AGG>
-__global__ void __launch_bounds__(256, (65536 / (256 * L::kRegCap)) > 0 ? 65536 / (256 * L::kRegCap) : 1)
-    k_atomic(LoopData d) {
+__device__ __forceinline__ void atomic_warp(const LoopData &d, uint32_t base) {
   using out_t = typename L::out_t;
   constexpr int D = L::kDim, K = L::kOut;
   const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
   out_t *__restrict__ out = static_cast<out_t *>(d.out);
-  for (uint32_t base = warp * 32u; base < d.n_cells; base += n_warps * 32u) {
-    const uint32_t c = base + lane;
-    const bool valid = c < d.n_cells;
-    GlobalRows<L, SOA> rows;
-    out_t inc[D][K];
+  const uint32_t c = base + lane;
+  const bool valid = c < d.n_cells;
+  GlobalRows<L, SOA> rows;
+  out_t inc[D][K];
 #pragma unroll
-    for (int s = 0; s < D; ++s) {
-      rows.p[0][s] = 0;
-      rows.p[1][s] = 0;
+  for (int s = 0; s < D; ++s) {
+    rows.p[0][s] = 0;
+    rows.p[1][s] = 0;
 #pragma unroll
-      for (int k = 0; k < K; ++k) inc[s][k] = out_t(0);
-    }
-    if (valid) {
-      load_row<D>(d.map[0], c, rows.p[0]);
-      if constexpr (L::kHasClass1) load_row<D>(d.map[1], c, rows.p[1]);
-      static_for_read<L>([&](auto r) {
-        constexpr int R = decltype(r)::value;
-        rows.base[R] = static_cast<const typename L::read_t *>(d.point[L::read_set(R)]);
-        rows.np[R] = d.n_points[L::read_set(R)];
-      });
-      Direct dir{d.cell, c, d.n_cells};
-      L::cell(rows, dir, inc);
-    }
+    for (int k = 0; k < K; ++k) inc[s][k] = out_t(0);
+  }
+  if (valid) {
+    load_row<D>(d.map[0], c, rows.p[0]);
+    if constexpr (L::kHasClass1) load_row<D>(d.map[1], c, rows.p[1]);
+    static_for_read<L>([&](auto r) {
+      constexpr int R = decltype(r)::value;
+      rows.base[R] = static_cast<const typename L::read_t *>(d.point[L::read_set(R)]);
+      rows.np[R] = d.n_points[L::read_set(R)];
+    });
+    Direct dir{d.cell, c, d.n_cells};
+    L::cell(rows, dir, inc);
+  }
 #pragma unroll
-    for (int s = 0; s < D; ++s) {
-      const uint32_t key = valid ? rows.p[0][s] : 0xFFFFFFFFu;
-      bool leader = valid;
-      if constexpr (AGG) {
-        const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
-        const unsigned lt = (1u << lane) - 1u;
-        const int rank = __popc(peers & lt);
-        const int cnt = __popc(peers);
-        const int maxcnt = (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)cnt);
-        for (int off = 1; off < maxcnt; off <<= 1) {
-          const bool has = rank + off < cnt;
-          const int src = has ? (int)__fns(peers, 0, rank + off + 1) : (int)lane;
-          const bool take = has && (rank % (2 * off)) == 0;
+  for (int s = 0; s < D; ++s) {
+    const uint32_t key = valid ? rows.p[0][s] : 0xFFFFFFFFu;
+    bool leader = valid;
+    if constexpr (AGG) {
+      const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
+      const unsigned lt = (1u << lane) - 1u;
+      const int rank = __popc(peers & lt);
+      const int cnt = __popc(peers);
+      const int maxcnt = (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)cnt);
+      for (int off = 1; off < maxcnt; off <<= 1) {
+        const bool has = rank + off < cnt;
+        const int src = has ? (int)__fns(peers, 0, rank + off + 1) : (int)lane;
+        const bool take = has && (rank % (2 * off)) == 0;
 #pragma unroll
-          for (int k = 0; k < K; ++k) {
-            const out_t v = __shfl_sync(0xFFFFFFFFu, inc[s][k], src);
-            if (take) inc[s][k] += v;
-          }
+        for (int k = 0; k < K; ++k) {
+          const out_t v = __shfl_sync(0xFFFFFFFFu, inc[s][k], src);
+          if (take) inc[s][k] += v;
         }
-        leader = valid && rank == 0;
       }
-      if (leader) {
-        if constexpr (!SOA && sizeof(out_t) == 4 && K == 4) {
-          float4 v = make_float4(inc[s][0], inc[s][1], inc[s][2], inc[s][3]);
-          atomicAdd(reinterpret_cast<float4 *>(out) + key, v);
-        } else {
+      leader = valid && rank == 0;
+    }
+    if (leader) {
+      if constexpr (!SOA && sizeof(out_t) == 4 && K == 4) {
+        float4 v = make_float4(inc[s][0], inc[s][1], inc[s][2], inc[s][3]);
+        atomicAdd(reinterpret_cast<float4 *>(out) + key, v);
+      } else {
 #pragma unroll
-          for (int k = 0; k < K; ++k)
-            atomic_add(out + out_index(SOA, d.n_points[0], key, K, k), inc[s][k]);
-        }
+        for (int k = 0; k < K; ++k)
+          atomic_add(out + out_index(SOA, d.n_points[0], key, K, k), inc[s][k]);
       }
     }
   }
+}
+
+template <class L, bool SOA, bool AGG>
+__global__ void __launch_bounds__(256, (65536 / (256 * L::kRegCap)) > 0 ? 65536 / (256 * L::kRegCap) : 1)
+    k_atomic(LoopData d) {
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t base = warp * 32u; base < d.n_cells; base += n_warps * 32u)
+    atomic_warp<L, SOA, AGG>(d, base);
 }
 
 } // namespace fot

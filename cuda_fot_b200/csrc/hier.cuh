@@ -280,7 +280,7 @@ constexpr int hier_min_blocks() {
 template <class L, bool SOA, int THREADS, bool STAGE>
 __global__ void __launch_bounds__(THREADS, hier_min_blocks<L, THREADS>())
     k_hier(LoopData d, HierPlanDev P) {
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   __shared__ TileMeta s_meta;
   __shared__ int s_abort;
   const uint32_t tid = threadIdx.x;
@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(THREADS, hier_min_blocks<L, THREADS>())
 template <class L, bool SOA, int THREADS, bool STAGE>
 __global__ void __launch_bounds__(THREADS, hier_min_blocks<L, THREADS>())
     k_hier_colour(LoopData d, HierPlanDev P, uint32_t first) {
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   __shared__ TileMeta s_meta;
   if (threadIdx.x == 0) s_meta = load_meta<L::kHasClass1>(P, first + blockIdx.x, 0);
   __syncthreads();

@@ -220,10 +220,10 @@ __device__ __forceinline__ void ws_stage_rows(const LoopData &d, const HierPlanD
   });
 }
 
-constexpr uint32_t kRecSlots = 3;
-
-template <class L, bool SOA, int T>
-// registers capped at the loop's kRegCap for every thread of the CTA
+// kRecSlots: tile-record slots (2 or 3; the plan picks 3 when the extra slot
+// costs no resident CTA).  Registers are capped at the loop's kRegCap for
+// every thread of the CTA.
+template <class L, bool SOA, int T, uint32_t kRecSlots>
 __global__ void __launch_bounds__(T + 64) __maxnreg__(L::kRegCap)
     k_hier_pipe(LoopData d, HierPlanDev P) {
   using out_t = typename L::out_t;
@@ -271,44 +271,30 @@ __global__ void __launch_bounds__(T + 64) __maxnreg__(L::kRegCap)
       uint32_t uses[kRecSlots] = {};  // copies issued per slot
       bool valid[kRecSlots] = {};
       uint32_t blk[kRecSlots] = {};
-      // claim pipeline: ticket t_a with its record offsets loaded, ticket t_b
-      // claimed one refill earlier
-      uint32_t t_a = atomicAdd(&P.ctl->ticket, 1u);
-      uint32_t t_b = atomicAdd(&P.ctl->ticket, 1u);
-      uint32_t a_off = 0, a_end = 0, a_err = 0;
-      auto load_a = [&]() {
-        if (t_a < P.total_tiles) {
-          const uint32_t b = t_a % P.n_blocks;
-          a_off = P.rec_off[b];
-          a_end = P.rec_off[b + 1];
-        }
-        a_err = *(volatile unsigned int *)&P.ctl->error;
-      };
+      // a slot is refilled with a freshly claimed tile: claiming only when a
+      // slot frees keeps few tiles claimed ahead of their dependencies
       bool more = true;
-      auto refill = [&](uint32_t s) {  // slot s gets ticket t_a
-        const bool ok = more && t_a < P.total_tiles && a_err == 0;
-        const uint32_t it = ok ? t_a / P.n_blocks : 0;
+      auto refill = [&](uint32_t s) {
+        const uint32_t t = more ? atomicAdd(&P.ctl->ticket, 1u) : P.total_tiles;
+        const bool ok = more && t < P.total_tiles && *(volatile unsigned int *)&P.ctl->error == 0;
+        const uint32_t it = ok ? t / P.n_blocks : 0;
+        const uint32_t b = ok ? t - it * P.n_blocks : 0;
         s_iter[s] = it;
         s_valid[s] = ok;
         valid[s] = ok;
-        blk[s] = ok ? t_a - it * P.n_blocks : 0;
+        blk[s] = b;
         if (ok) {
+          const uint32_t off = P.rec_off[b], end = P.rec_off[b + 1];
           // the slot was last read through the generic proxy
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          mbar_expect_tx(&s_rec_full[s], a_end - a_off);
-          bulk_copy_g2s(rec_base + s * P.rec_slot, P.rec + a_off, a_end - a_off, &s_rec_full[s]);
+          mbar_expect_tx(&s_rec_full[s], end - off);
+          bulk_copy_g2s(rec_base + s * P.rec_slot, P.rec + off, end - off, &s_rec_full[s]);
         } else {
           mbar_arrive(&s_rec_full[s]);
           more = false;
         }
         ++uses[s];
-        t_a = t_b;
-        if (more) {
-          load_a();
-          t_b = atomicAdd(&P.ctl->ticket, 1u);
-        }
       };
-      load_a();
       for (uint32_t s = 0; s < kRecSlots && more; ++s) refill(s);
       for (uint32_t j = 0;; ++j) {
         const uint32_t s = j % kRecSlots;
@@ -318,12 +304,11 @@ __global__ void __launch_bounds__(T + 64) __maxnreg__(L::kRegCap)
           s_stop = 1;
           break;
         }
-        const uint32_t done_block = blk[s], done_it = base + s_iter[s] + 1;
-        if (more) refill(s);
-        else valid[s] = false;
         // the compute threads' stores (ordered before this thread by the
         // mbarrier) become visible before the flag
-        st_release_gpu(P.block_done + done_block, done_it);
+        st_release_gpu(P.block_done + blk[s], base + s_iter[s] + 1);
+        if (more) refill(s);
+        else valid[s] = false;
       }
       // let every record copy still in flight land (bounded)
       for (uint32_t s = 0; s < kRecSlots; ++s)

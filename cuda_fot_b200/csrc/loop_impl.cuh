@@ -41,11 +41,11 @@ template <bool SOA, bool STAGE> const void *hier_kernel_t(bool persistent, uint3
   return nullptr;
 }
 
-template <bool SOA> const void *pipe_kernel(uint32_t threads) {
+template <bool SOA, uint32_t SLOTS> const void *pipe_kernel(uint32_t threads) {
   switch (threads) {
-  case 128: return reinterpret_cast<const void *>(&k_hier_pipe<L, SOA, 128>);
-  case 256: return reinterpret_cast<const void *>(&k_hier_pipe<L, SOA, 256>);
-  case 512: return reinterpret_cast<const void *>(&k_hier_pipe<L, SOA, 512>);
+  case 128: return reinterpret_cast<const void *>(&k_hier_pipe<L, SOA, 128, SLOTS>);
+  case 256: return reinterpret_cast<const void *>(&k_hier_pipe<L, SOA, 256, SLOTS>);
+  case 512: return reinterpret_cast<const void *>(&k_hier_pipe<L, SOA, 512, SLOTS>);
   }
   return nullptr;
 }
@@ -55,8 +55,10 @@ const void *kernel_for(int exec, bool soa, uint32_t threads, uint32_t variant) {
   if (exec == FOT_EXEC_ATOMIC)
     return soa ? reinterpret_cast<const void *>(&k_atomic<L, true, true>)
                : reinterpret_cast<const void *>(&k_atomic<L, false, true>);
-  if (exec == FOT_EXEC_HIER && (variant & kVariantPipe))
-    return soa ? pipe_kernel<true>(threads) : pipe_kernel<false>(threads);
+  if (exec == FOT_EXEC_HIER && (variant & kVariantPipe)) {
+    if (variant & kVariantSlots3) return soa ? pipe_kernel<true, 3>(threads) : pipe_kernel<false, 3>(threads);
+    return soa ? pipe_kernel<true, 2>(threads) : pipe_kernel<false, 2>(threads);
+  }
   const bool persistent = exec == FOT_EXEC_HIER;
   const bool stage = variant & 1u;
   if (soa) return stage ? hier_kernel_t<true, true>(persistent, threads)
@@ -111,11 +113,11 @@ void smem_layout(uint32_t cap0, uint32_t cap1, uint32_t variant, uint32_t rec_ca
   SmemLayout s;
   size_t off = 0;
   if (variant & kVariantPipe) {
-    // kRecSlots tile-record slots, 2 read-row slots, the per-slot increments, 2
+    // 2 or 3 tile-record slots, 2 read-row slots, the per-slot increments, 2
     // prefetched-output-row slots (AOS output rows of a multiple of 16 bytes)
     auto a128 = [](size_t v) { return (v + 127) & ~size_t(127); };
     s.rec_slot = (uint32_t)a128(rec_cap);
-    off = kRecSlots * (size_t)s.rec_slot;
+    off = ((variant & kVariantSlots3) ? 3 : 2) * (size_t)s.rec_slot;
     s.rows_off = (uint32_t)off;
     size_t rows = 0;
     for (int r = 0; r < L::kNumRead; ++r) {

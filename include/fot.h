@@ -245,8 +245,13 @@ int fot_graph_destroy(fot_graph *g);
 
 /* ---- batches: many meshes, one persistent launch -------------------------- */
 
-/* Group hierarchical plans of several problems into one persistent launch
- * over a (mesh, block) tile queue ordered by block colour per mesh. */
+/* Group the plans of several problems into one launch per fot_batch_run.
+ * Hierarchical plans: one persistent launch over a (mesh, block) tile queue
+ * ordered by block colour per mesh; each mesh's result is that of its own
+ * plan.  Atomic plans (all with or all without warp aggregation): one launch
+ * over tiles of 1,024 cells of every mesh and every iteration.  A batch holds
+ * one executor kind, one layout, and one loop kind or res_calc with volna.
+ * No counterpart in the reference (one mesh per process). */
 int fot_batch_create(fot_problem *const *problems, fot_plan *const *plans,
                      uint32_t n, fot_batch **out);
 int fot_batch_run(fot_batch *b, uint32_t iterations, void *stream);

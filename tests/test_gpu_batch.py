@@ -1,11 +1,12 @@
-"""GPU parity of the batched persistent executor (fot_batch): many meshes of
-uneven size in ONE launch over a (mesh, block colour) tile queue.
+"""GPU parity of the batched executors (fot_batch): many meshes of uneven
+size in ONE launch.
 
-Each mesh's tiles run in its own plan's colour order, with the thread-colour
-accumulation of the hierarchical executor, so every mesh's result is
-BIT-IDENTICAL to the oracle's CPU replay of its own plan, and within 1e-12
-(FP64) / 1e-5 (FP32 volna) of the serial loop.  A CUDA graph of batched
-launches equals the same launches issued directly.
+Hierarchical plans: each mesh's tiles run in its own plan's colour order,
+with the thread-colour accumulation of the hierarchical executor, so every
+mesh's result is BIT-IDENTICAL to the oracle's CPU replay of its own plan,
+and within 1e-12 (FP64) / 1e-5 (FP32 volna) of the serial loop; a CUDA graph
+of batched launches equals the same launches issued directly.  Atomic plans:
+every mesh within the same tolerances of its serial loop.
 """
 import numpy as np
 import pytest
@@ -98,10 +99,41 @@ def test_batch_graph_equals_direct_launches():
     del g
 
 
-def test_batch_rejects_atomic_plans_and_mixed_kinds():
+@pytest.mark.parametrize("aggregate", [True, False])
+def test_atomic_batch_matches_serial(aggregate):
+    """Atomic plans of many meshes in one launch: each mesh within the
+    atomic tolerance of its serial loop (summation order is not fixed)."""
+    mds = mixed_meshes()
+    probs = [F().Problem.from_mesh(md) for md in mds]
+    flags = 0 if aggregate else F().PLAN_NO_AGGREGATE
+    b = F().Batch([p.plan(F().EXEC_ATOMIC, 256, flags) for p in probs])
+    b.run(2)
+    b.run(1)
+    b.sync()
+    for md, p in zip(mds, probs):
+        ser, _ = O.serial(md, 3)
+        assert rel_err(p.point_weights(0), ser[0]) <= tol(md.loop), (mg.LOOP_NAMES[md.loop], md.n_cells)
+
+
+@pytest.mark.parametrize("loop", [mg.MINI_AERO, mg.LULESH, mg.GETACC])
+def test_single_kind_atomic_batch_matches_serial(loop):
+    mds = single_kind(loop)
+    probs = [F().Problem.from_mesh(md) for md in mds]
+    b = F().Batch([p.plan(F().EXEC_ATOMIC, 256) for p in probs])
+    b.run(3)
+    b.sync()
+    for md, p in zip(mds, probs):
+        ser, ser_cd = O.serial(md, 3)
+        assert rel_err(p.point_weights(0), ser[0]) <= tol(md.loop)
+        for j, ref in enumerate(ser_cd):  # lulesh's written element volumes
+            assert bitwise_equal(p.cell_weights(j), ref)
+
+
+def test_batch_rejects_mixed_executors_and_kinds():
     md1, md2 = mg.res_calc(6, 5, 1), mg.lulesh(3, 2)
     p1, p2 = F().Problem.from_mesh(md1), F().Problem.from_mesh(md2)
+    p3 = F().Problem.from_mesh(mg.res_calc(7, 5, 3))
     with pytest.raises(F().FotError):
-        F().Batch([p1.plan(F().EXEC_ATOMIC, 256)])
+        F().Batch([p1.plan(F().EXEC_ATOMIC, 256), p3.plan(F().EXEC_HIER, 64)])
     with pytest.raises(F().FotError):
         F().Batch([p1.plan(F().EXEC_HIER, 64), p2.plan(F().EXEC_HIER, 64)])
