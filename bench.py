@@ -247,27 +247,41 @@ def main(argv=None):
     ub = md.unique_bytes()
     stream = torch.cuda.current_stream()
 
-    # plan choice: the cost model's pick when available, else the measured sweep
+    # plan choice: the cost model's pick when a trained model is present, else
+    # the measured sweep; the sweep also judges the model's pick (regret)
+    from cuda_fot_b200.profile_case import parse_plan
     choice_src = "sweep"
+    choice_note = None
     chosen = None
+    pick_s = None
     try:
         from cuda_fot_b200 import costmodel as CM
         model = CM.load_default()
         if model is not None:
+            t_pick = time.perf_counter()
             chosen = CM.pick(model, md, T.default_candidates(md.loop))
+            pick_s = time.perf_counter() - t_pick
             choice_src = "cost model"
-    except Exception:
+        else:
+            choice_note = "no trained model (cuda_fot_b200/model/costmodel.npz)"
+    except Exception as e:  # the measured sweep stays the fallback
         chosen = None
+        choice_note = f"cost model unavailable: {e}"
     cache = T.OrderedCache(md)
-    sweep_res = []
     if args.plan:
-        o, e, b = args.plan.split("/")
-        chosen = T.Candidate(None if o == "as-is" else o, 0, e, int(b))
+        chosen = parse_plan(args.plan)
         choice_src = "forced"
-    if chosen is None:
-        for c in T.default_candidates(md.loop, quick=True):
+    sweep_res = []
+    if choice_src != "forced":
+        cands = T.default_candidates(md.loop, quick=True)
+        if chosen is not None and chosen.label() not in [c.label() for c in cands]:
+            cands.append(chosen)
+        t_sweep = time.perf_counter()
+        for c in cands:
             sweep_res.append(T.measure(cache, c, iters=5, warmup=3))
-        chosen = T.best(sweep_res)["cand"]
+        sweep_s = time.perf_counter() - t_sweep
+        if chosen is None:
+            chosen = T.best(sweep_res)["cand"]
     atomic_plain = T.measure(cache, T.Candidate(None, 0, "atomic", 256, aggregate=False),
                              iters=10, warmup=3)
 
@@ -374,6 +388,13 @@ def main(argv=None):
         }
         if sweep_res:
             line["sweep"] = {r["cand"].label(): (round(r["gbs"], 1) if r["ok"] else None) for r in sweep_res}
+            best = T.best(sweep_res)
+            mine = next((r for r in sweep_res if r["cand"].label() == chosen.label() and r["ok"]), None)
+            line["plan_judge"] = {"sweep_best": best["cand"].label(), "sweep_s": round(sweep_s, 1),
+                                  "model_pick_s": round(pick_s, 1) if pick_s is not None else None,
+                                  "regret": (mine["seconds"] / best["seconds"] - 1.0) if mine else None}
+        if choice_note:
+            line["plan_note"] = choice_note
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

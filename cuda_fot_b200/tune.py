@@ -56,6 +56,9 @@ def default_candidates(loop: int, quick: bool = False) -> List[Candidate]:
     out = []
     for o in orders:
         out.append(Candidate(o, 0, "atomic", 256))
+        if not quick:
+            out.append(Candidate(o, 0, "atomic", 256, aggregate=False))
+            out.append(Candidate(o, 0, "hier", 128, True))
         for b in blocks:
             out.append(Candidate(o, 0, "hier", b))
     if not quick:
