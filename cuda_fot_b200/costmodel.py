@@ -2,7 +2,8 @@
 
 A 24 -> 64 -> 64 -> 1 MLP (libfot's fot_model_* kernels: forward, backward
 and Adam on the GPU) predicts log(seconds per iteration) of a candidate plan
-(ordering, partition, executor, block size; cuda_fot_b200.tune.Candidate) from
+(ordering, partition, executor, block size; cuda_fot_b200.tune.Candidate),
+relative to the mean over the candidates timed on the same mesh, from
 features of the mesh AFTER the candidate's ordering and of the plan.  The
 autotuner's exhaustive measured sweep generates the training data and stays
 as the fallback and the judge: the model's pick is compared with the sweep's
@@ -363,6 +364,18 @@ def pick(model: CostModel, md: mg.MeshData, candidates: List[T.Candidate]) -> T.
 DEFAULT_SIZES = (1e4, 4e4, 1.6e5, 6.4e5, 2.5e6, 1e7)
 
 
+def centred_targets(y: np.ndarray, group: np.ndarray) -> np.ndarray:
+    """log time minus the mean log time of its mesh group.  A plan choice
+    only compares candidates on one mesh, so the model learns each plan's
+    time relative to the other plans on that mesh; the mesh-level constant
+    (which the features would otherwise have to explain) drops out."""
+    t = np.asarray(y, np.float64).copy()
+    for g in np.unique(group):
+        idx = group == g
+        t[idx] -= t[idx].mean()
+    return t.astype(np.float32)
+
+
 def train_and_evaluate(data: dict, holdout_seed: Optional[int] = None, epochs: int = 200,
                        seed: int = 1) -> tuple:
     """Train on every seed but the held-out one (default: the largest) and
@@ -375,7 +388,8 @@ def train_and_evaluate(data: dict, holdout_seed: Optional[int] = None, epochs: i
     train = seeds != hold
     m = CostModel(seed=seed)
     t0 = time.time()
-    losses = m.fit(data["X"][train], data["y"][train], epochs=epochs, batch=256, lr=2e-3)
+    t = centred_targets(data["y"], data["group"])
+    losses = m.fit(data["X"][train], t[train], epochs=epochs, batch=256, lr=2e-3)
     train_s = time.time() - t0
     ev = evaluate(m, data, ~train)
     held = [d for d in info if d["seed"] == hold]
