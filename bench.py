@@ -5,7 +5,8 @@ timed steps run as one Plan.run(K) call, as the reference's
 Problem::loop*(num) runs and times `num` iterations per call):
 mini_aero-style 3D face flux, FP64, 128^3 hex cells, 6,242,304 interior faces,
 cell numbering a seeded random permutation; the plan (ordering + executor +
-block size) is picked by the cost model when one is trained and available,
+block size + point-data layout, AOS or SOA as the reference's Problem<SOA>)
+is picked by the cost model when one is trained and available,
 otherwise by the measured sweep of the autotuner.  GB/s counts the algorithmic
 ("unique") bytes of one step: every indirectly read dataset once, the
 incremented dataset read and written once, every direct dataset once, the
@@ -285,7 +286,7 @@ def main(argv=None):
     atomic_plain = T.measure(cache, T.Candidate(None, 0, "atomic", 256, aggregate=False),
                              iters=10, warmup=3)
 
-    md_run = cache.get(chosen.order, chosen.partition)
+    md_run = cache.get(chosen.order, chosen.partition, chosen.layout)
     p, plan = T.build(md_run, chosen)
     # launches of one Plan.run(K) call: the atomic executor launches once per
     # iteration, the persistent hierarchical kernel once per call, the
@@ -369,6 +370,7 @@ def main(argv=None):
                        "unique_bytes_per_step": ub, "seed": args.seed,
                        "l2": "inputs larger than L2 (%.2f GB per step vs 126 MB L2)" % (ub / 1e9),
                        "plan": chosen.label(), "plan_choice": choice_src,
+                       "point_layout": chosen.layout.upper(),
                        "n_blocks": st["n_blocks"], "block_colours": st["n_colours"],
                        "timed_call": f"Plan.run({args.steps}): {args.steps} iterations in one call",
                        "parallelism": f"replicas x{world}"},

@@ -2,7 +2,8 @@
 
 A 24 -> 64 -> 64 -> 1 MLP (libfot's fot_model_* kernels: forward, backward
 and Adam on the GPU) predicts log(seconds per iteration) of a candidate plan
-(ordering, partition, executor, block size; cuda_fot_b200.tune.Candidate),
+(ordering, partition, executor, block size, point layout;
+cuda_fot_b200.tune.Candidate),
 relative to the mean over the candidates timed on the same mesh, from
 features of the mesh AFTER the candidate's ordering and of the plan.  The
 autotuner's exhaustive measured sweep generates the training data and stays
@@ -35,13 +36,13 @@ DEFAULT_MODEL = os.path.join(MODEL_DIR, "costmodel.npz")
 DEFAULT_CORPUS = os.path.join(MODEL_DIR, "corpus.npz")
 
 FEATURES = [
-    "log10_cells", "log10_points", "mesh_dim", "out_dim", "log10_unique_bytes",
+    "log10_cells", "log10_points", "mesh_dim", "log10_unique_bytes",
     "read_bytes_per_cell/100", "direct_bytes_per_cell/100",
     "loop_res_calc", "loop_mini_aero", "loop_lulesh", "loop_volna", "loop_getacc",
     "deg_le2", "deg_3_4", "deg_5_6", "deg_ge7",
     "log10_1p_bandwidth", "log10_1p_mean_span",
     "exec_atomic", "exec_hier", "exec_hier_launch", "log2_block", "partitioned",
-    "direct_reads_or_plain_atomics",
+    "direct_reads_or_plain_atomics", "soa_layout",
 ]
 assert len(FEATURES) == N_FEATURES
 
@@ -50,7 +51,8 @@ _fp = C.POINTER(C.c_float)
 
 
 def mesh_features(md: mg.MeshData) -> np.ndarray:
-    """17 features of a mesh in its current numbering."""
+    """16 features of a mesh in its current numbering (the loop's output
+    dimension is implied by the loop's one-hot)."""
     m0 = np.asarray(md.maps[0])
     n, dim = m0.shape
     np0 = md.n_points[0]
@@ -72,22 +74,24 @@ def mesh_features(md: mg.MeshData) -> np.ndarray:
     onehot = np.zeros(5)
     onehot[md.loop] = 1
     f = np.concatenate([
-        [np.log10(n), np.log10(np0), dim, info.point_dim[0], np.log10(md.unique_bytes()),
+        [np.log10(n), np.log10(np0), dim, np.log10(md.unique_bytes()),
          read_bytes / 100.0, direct / 100.0], onehot, hist,
         [np.log10(1 + span.max()), np.log10(1 + span.mean())]])
     return f.astype(np.float32)
 
 
 def plan_features(c: T.Candidate) -> np.ndarray:
-    """7 plan features; the last one is 1 for direct (unstaged) reads of a
-    hierarchical plan and for an atomic plan without warp aggregation."""
+    """8 plan features; the seventh is 1 for direct (unstaged) reads of a
+    hierarchical plan and for an atomic plan without warp aggregation, the
+    last 1 for SOA point data."""
     ex = np.zeros(3)
     ex[["atomic", "hier", "hier_launch"].index(c.exec)] = 1
     if c.exec == "atomic":
-        last = 0.0 if c.aggregate else 1.0
+        var = 0.0 if c.aggregate else 1.0
     else:
-        last = 1.0 if c.direct else 0.0
-    return np.concatenate([ex, [np.log2(c.block), 1.0 if c.partition else 0.0, last]]).astype(np.float32)
+        var = 1.0 if c.direct else 0.0
+    return np.concatenate([ex, [np.log2(c.block), 1.0 if c.partition else 0.0, var,
+                                1.0 if c.layout == "soa" else 0.0]]).astype(np.float32)
 
 
 def features(mesh_f: np.ndarray, c: T.Candidate) -> np.ndarray:
@@ -180,23 +184,29 @@ class CostModel:
 
 
 def load_default() -> Optional[CostModel]:
-    if os.path.exists(DEFAULT_MODEL):
-        return CostModel.load(DEFAULT_MODEL)
-    return None
+    """The committed model, or None when there is none or it was trained on
+    another feature list (then the measured sweep chooses)."""
+    if not os.path.exists(DEFAULT_MODEL):
+        return None
+    z = np.load(DEFAULT_MODEL)
+    if "features" not in z.files or [str(f) for f in z["features"]] != FEATURES:
+        return None
+    return CostModel.load(DEFAULT_MODEL)
 
 
 # ---------------------------------------------------------------------------
 # training data: measured sweeps over seeded synthetic meshes
 # ---------------------------------------------------------------------------
 def corpus_candidates(loop: int) -> List[T.Candidate]:
-    """Plan candidates of one (mesh, ordering): executors x block sizes x
-    staging; partitioned variants are separate orderings."""
-    out = [T.Candidate(None, 0, "atomic", 256), T.Candidate(None, 0, "atomic", 256, aggregate=False)]
-    for b in (64, 128, 256, 512):
-        out.append(T.Candidate(None, 0, "hier", b, False))
-        out.append(T.Candidate(None, 0, "hier", b, True))
-    out.append(T.Candidate(None, 0, "hier_launch", 256, False))
-    out.append(T.Candidate(None, 0, "hier_launch", 256, True))
+    """Plan candidates of one (mesh, ordering): point layouts x executors x
+    block sizes x staging; partitioned variants are separate orderings."""
+    out = []
+    for lay in ("aos", "soa"):
+        out.append(T.Candidate(None, 0, "atomic", 256, layout=lay))
+        out.append(T.Candidate(None, 0, "atomic", 256, aggregate=False, layout=lay))
+        for b in (128, 256, 512):
+            out.append(T.Candidate(None, 0, "hier", b, False, layout=lay))
+        out.append(T.Candidate(None, 0, "hier", 128, True, layout=lay))
     return out
 
 
@@ -256,11 +266,11 @@ def generate(loops: Sequence[int], sizes: Sequence[float], seeds: Sequence[int],
                             if c.exec != "atomic" and c.block != 256:
                                 continue
                             blk = 256 if c.exec == "atomic" else part
-                            c = T.Candidate(order, part, c.exec, blk, c.direct, c.aggregate)
+                            c = T.Candidate(order, part, c.exec, blk, c.direct, c.aggregate, c.layout)
                         else:
-                            c = T.Candidate(order, 0, c.exec, c.block, c.direct, c.aggregate)
+                            c = T.Candidate(order, 0, c.exec, c.block, c.direct, c.aggregate, c.layout)
                         try:
-                            p, plan = T.build(mdo, c)
+                            p, plan = T.build(cache.get(order, part, c.layout), c)
                             t1 = T.time_plan(p, plan, iters=2, warmup=1)
                             iters = int(min(50, max(3, iters_min_ms * 1e-3 / max(t1, 1e-7))))
                             secs = T.time_plan(p, plan, iters=iters, warmup=1)

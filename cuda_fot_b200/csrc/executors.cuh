@@ -18,12 +18,15 @@
 //     zeroed shared accumulator in thread-colour order (one __syncthreads per
 //     thread colour) and finally adds the accumulator to point dataset 0 in
 //     HBM.  Blocks of one block colour write disjoint points.  In the
-//     persistent form (FOT_EXEC_HIER) CTAs claim tiles from a queue stored in
-//     block-colour order (and iteration after iteration); a tile computes
+//     persistent forms (FOT_EXEC_HIER) CTAs claim tiles from a queue stored
+//     in block-colour order (and iteration after iteration); a tile computes
 //     immediately -- the loops never read the dataset they increment -- and
-//     only its write-back waits, with a bounded spin, until every tile of the
-//     earlier colours has written back.  The result is therefore
-//     deterministic and equal to replaying the colours in order on the CPU.
+//     only its write-back waits, with a bounded spin, until what it conflicts
+//     with has been written back: every tile of the earlier colours for the
+//     simple kernel (k_hier, hier.cuh), the conflicting blocks' completion
+//     flags for the pipelined warp-specialised kernel (k_hier_pipe,
+//     hier_pipe.cuh, the default).  The result is therefore deterministic
+//     and equal to replaying the colours in order on the CPU.
 #pragma once
 
 #include <cstdint>

@@ -6,8 +6,8 @@
 Builds the mesh and the plan, then calls Plan.run(1) `--launches` times, so a
 profiler can skip the first launches (-s) and capture one to three (-c) of the
 same kernel.  Plan labels are those of cuda_fot_b200.tune.Candidate.label():
-`order[+partN]/exec[d][-plain]/block`, e.g. `gps/hier/128`, `gps+part256/hierd/256`,
-`as-is/atomic-plain/256`.  Sizes: res_calc/volna/getacc take --n as the grid edge
+`order[+partN]/exec[d][-plain]/block[@soa]`, e.g. `gps/hier/128`,
+`gps+part256/hierd/256`, `as-is/atomic-plain/256@soa`.  Sizes: res_calc/volna/getacc take --n as the grid edge
 (n x n), mini_aero/lulesh as the hex edge (n^3).
 """
 from __future__ import annotations
@@ -20,6 +20,9 @@ from . import tune as T
 
 
 def parse_plan(label: str) -> T.Candidate:
+    layout = "aos"
+    if label.endswith("@soa"):
+        label, layout = label[: -len("@soa")], "soa"
     order, ex, block = label.split("/")
     part = 0
     if "+part" in order:
@@ -33,7 +36,7 @@ def parse_plan(label: str) -> T.Candidate:
     if ex in ("hierd", "hier_launchd"):
         direct = True
         ex = ex[:-1]
-    return T.Candidate(None if order == "as-is" else order, part, ex, int(block), direct, aggregate)
+    return T.Candidate(None if order == "as-is" else order, part, ex, int(block), direct, aggregate, layout)
 
 
 def make_mesh(loop: str, n: int, seed: int) -> mg.MeshData:
@@ -61,7 +64,7 @@ def main(argv=None) -> int:
     md = make_mesh(a.loop, a.n, a.seed)
     cand = parse_plan(a.plan)
     cache = T.OrderedCache(md)
-    p, plan = T.build(cache.get(cand.order, cand.partition), cand)
+    p, plan = T.build(cache.get(cand.order, cand.partition, cand.layout), cand)
     for _ in range(a.launches):
         plan.run(1)
     p.sync()

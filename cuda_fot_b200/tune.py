@@ -1,6 +1,6 @@
 """Autotuner: candidate plans and their measured timings.
 
-A candidate is (ordering, partition size, executor, block size):
+A candidate is (ordering, partition size, executor, block size, layout):
 
 * ordering  -- None (keep the numbering), "natural" (cells sorted by point
   tuple), "random", "rcm" or "gps" (fot_reorder);
@@ -8,7 +8,8 @@ A candidate is (ordering, partition size, executor, block size):
   fot_reorder_to_partition and fot_renumber_points (the reference's
   partition -> reorderToPartition -> renumberPoints sequence);
 * executor  -- "atomic", "hier" (persistent) or "hier_launch";
-* block     -- cells per block (hierarchical) / threads per CTA (atomic).
+* block     -- cells per block (hierarchical) / threads per CTA (atomic);
+* layout    -- "aos" or "soa" point data (the reference's Problem<SOA>).
 
 ``measure(md, cand)`` builds the candidate on a fresh problem and times
 ``iters`` iterations with CUDA events on the launching stream after warm-up.
@@ -41,30 +42,33 @@ class Candidate:
     block: int = 256
     direct: bool = False  # hierarchical: gather read rows from HBM/L2 (no staging)
     aggregate: bool = True  # atomic: warp aggregation of same-target lanes
+    layout: str = "aos"     # point-data layout of the problem the plan runs on
 
     def label(self) -> str:
         o = self.order or "as-is"
         p = f"+part{self.partition}" if self.partition else ""
         d = "d" if self.direct and self.exec != "atomic" else ""
         a = "-plain" if self.exec == "atomic" and not self.aggregate else ""
-        return f"{o}{p}/{self.exec}{d}{a}/{self.block}"
+        lay = "@soa" if self.layout == "soa" else ""
+        return f"{o}{p}/{self.exec}{d}{a}/{self.block}{lay}"
 
 
 def default_candidates(loop: int, quick: bool = False) -> List[Candidate]:
     orders = ["gps", "rcm"] if quick else [None, "random", "rcm", "gps"]
     blocks = [128, 256] if quick else [128, 256, 512]
     out = []
-    for o in orders:
-        out.append(Candidate(o, 0, "atomic", 256))
+    for lay in ("aos", "soa"):
+        for o in orders:
+            out.append(Candidate(o, 0, "atomic", 256, layout=lay))
+            out.append(Candidate(o, 0, "atomic", 256, aggregate=False, layout=lay))
+            if not quick:
+                out.append(Candidate(o, 0, "hier", 128, True, layout=lay))
+            for b in blocks:
+                out.append(Candidate(o, 0, "hier", b, layout=lay))
         if not quick:
-            out.append(Candidate(o, 0, "atomic", 256, aggregate=False))
-            out.append(Candidate(o, 0, "hier", 128, True))
-        for b in blocks:
-            out.append(Candidate(o, 0, "hier", b))
-    if not quick:
-        for b in blocks:
-            out.append(Candidate("gps", b, "hier", b))
-            out.append(Candidate("rcm", b, "hier", b))
+            for b in blocks:
+                out.append(Candidate("gps", b, "hier", b, layout=lay))
+                out.append(Candidate("rcm", b, "hier", b, layout=lay))
     return out
 
 
@@ -76,7 +80,12 @@ class OrderedCache:
         self.md = md
         self._cache: Dict = {}
 
-    def get(self, order: Optional[str], partition: int) -> mg.MeshData:
+    def get(self, order: Optional[str], partition: int, layout: Optional[str] = None) -> mg.MeshData:
+        if layout is not None and layout != self.md.layout:
+            key = (order, partition, layout)
+            if key not in self._cache:
+                self._cache[key] = self.get(order, partition).to_layout(layout)
+            return self._cache[key]
         key = (order, partition)
         if key not in self._cache:
             p = F.Problem.from_mesh(self.md)
@@ -97,7 +106,10 @@ class OrderedCache:
 
 
 def build(md: mg.MeshData, cand: Candidate, stream=None):
-    """A problem holding md (already ordered) and the candidate's plan."""
+    """A problem holding md (already ordered; converted to the candidate's
+    layout when it is not in it) and the candidate's plan."""
+    if md.layout != cand.layout:
+        md = md.to_layout(cand.layout)
     p = F.Problem.from_mesh(md)
     flags = 0
     if cand.partition:
@@ -129,7 +141,7 @@ def time_plan(p, plan, iters: int = 10, warmup: int = 3, stream=None) -> float:
 
 
 def measure(cache: OrderedCache, cand: Candidate, iters: int = 10, warmup: int = 3) -> dict:
-    md = cache.get(cand.order, cand.partition)
+    md = cache.get(cand.order, cand.partition, cand.layout)
     try:
         t0 = time.perf_counter()
         p, plan = build(md, cand)

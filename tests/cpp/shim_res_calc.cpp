@@ -5,6 +5,9 @@
 // hierarchical or global loop and writes the un-permuted result.
 //
 //   shim_res_calc <dir> <iterations> <exec: hier|global> <reorder: 0|1> <out>
+//
+// Built with -DSHIM_SOA=1 it runs Problem<true> (component-major point data);
+// the text files are point-major in both layouts, as the reference's readers.
 #include <fstream>
 #include <iostream>
 #include <string>
@@ -12,6 +15,10 @@
 #include "fot_problem.hpp"
 
 using fot::compat::Problem;
+
+#ifndef SHIM_SOA
+#define SHIM_SOA 0
+#endif
 
 int main(int argc, char **argv) {
   if (argc < 6) return 2;
@@ -22,7 +29,7 @@ int main(int argc, char **argv) {
   try {
     std::ifstream mesh_res(dir + "/mesh_res"), mesh_x(dir + "/mesh_x"), mesh_q(dir + "/mesh_q"),
         mesh_adt(dir + "/mesh_adt");
-    Problem<false> problem({&mesh_res, &mesh_x, &mesh_q, &mesh_adt}, {2, 2, 2, 2},
+    Problem<SHIM_SOA != 0> problem({&mesh_res, &mesh_x, &mesh_q, &mesh_adt}, {2, 2, 2, 2},
                            {{4, sizeof(double)}, {2, sizeof(double)}, {4, sizeof(double)},
                             {1, sizeof(double)}},
                            {}, 128);

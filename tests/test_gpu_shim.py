@@ -25,11 +25,12 @@ def write_inputs(md, d):
             np.savetxt(f, md.point_data[k], fmt="%.17g")
 
 
-@pytest.fixture(scope="module")
-def driver(tmp_path_factory):
-    out = tmp_path_factory.mktemp("shim") / "shim_res_calc"
+@pytest.fixture(scope="module", params=["aos", "soa"])
+def driver(request, tmp_path_factory):
+    out = tmp_path_factory.mktemp("shim") / f"shim_res_calc_{request.param}"
     lib = os.path.join(ROOT, "cuda_fot_b200")
     subprocess.run(["g++", "-std=c++17", "-O2", "-I" + os.path.join(ROOT, "include"),
+                    "-DSHIM_SOA=%d" % (request.param == "soa"),
                     os.path.join(ROOT, "tests", "cpp", "shim_res_calc.cpp"), "-o", str(out),
                     "-L" + lib, "-lfot", "-Wl,-rpath," + lib], check=True)
     return str(out)
