@@ -257,14 +257,14 @@ def main(argv=None):
     pick_s = None
     try:
         from cuda_fot_b200 import costmodel as CM
-        model = CM.load_default()
+        model = None if args.plan else CM.load_default()  # a forced plan needs no pick
         if model is not None:
             t_pick = time.perf_counter()
             chosen = CM.pick(model, md, T.default_candidates(md.loop))
             pick_s = time.perf_counter() - t_pick
             choice_src = "cost model"
-        else:
-            choice_note = "no trained model (cuda_fot_b200/model/costmodel.npz)"
+        elif not args.plan:
+            choice_note = "no trained model for the current features (cuda_fot_b200/model/costmodel.npz)"
     except Exception as e:  # the measured sweep stays the fallback
         chosen = None
         choice_note = f"cost model unavailable: {e}"
@@ -353,7 +353,7 @@ def main(argv=None):
     peak, peak_src = load_peaks()
     # algorithmic bytes per iteration / device time per iteration of this rank
     achieved = ub / (secs / args.steps) / 1e9
-    kernel_key = f"{chosen.exec}"
+    kernel_key = chosen.label().split("/", 1)[1]  # kernel variant: executor, block, layout
     traffic, traffic_src = load_traffic(kernel_key)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
