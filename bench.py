@@ -126,9 +126,13 @@ def dist_setup(gpus):
         rank = int(os.environ.get("RANK", "0"))
         world = int(os.environ.get("WORLD_SIZE", "1"))
         local = int(os.environ.get("LOCAL_RANK", "0"))
-        torch.cuda.set_device(local)
+        # one process per GPU over NCCL; gloo where no GPU is visible (the
+        # host-side tests of the replica path)
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
         return rank, world, local
     return 0, 1, 0
 
@@ -144,7 +148,8 @@ def max_over_ranks(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
