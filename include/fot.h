@@ -283,7 +283,8 @@ int fot_model_predict(fot_model *m, const float *X, int n, float *y);
  * reference).  For callers that must not allocate device memory once they
  * are running: the inputs and outputs of the call are staged in a fixed
  * file-scope device array of FOT_MODEL_NOALLOC_MAX_ROWS rows (25 floats per
- * row, 409,600 bytes) instead of buffers allocated per call.  More rows
+ * row, 409,600 bytes, held on every GPU that loads the library until the
+ * process exits) instead of buffers allocated per call.  More rows
  * than that: FOT_ERR_LIMIT, nothing is computed.  No part of the array has
  * to start at zero (a call writes every row it reads).  All calls on one
  * device share the array, so calls that overlap in time (from several host
