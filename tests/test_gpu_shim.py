@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 from cuda_fot_b200 import meshgen as mg
+from cuda_fot_b200 import textio
 from oracle import oracle_py as O
 from tests.helpers import rel_err
 
@@ -16,13 +17,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def write_inputs(md, d):
-    names = ["res", "x", "q", "adt"]
-    for k, name in enumerate(names):
-        with open(os.path.join(d, f"mesh_{name}"), "w") as f:
-            f.write(f"{md.n_points[k]} {md.n_cells}\n")
-            np.savetxt(f, md.maps[k], fmt="%d")
-        with open(os.path.join(d, f"data_{name}"), "w") as f:
-            np.savetxt(f, md.point_data[k], fmt="%.17g")
+    # the reference's res_calc input files: mesh_<name> and data_<name>
+    textio.save_mesh_data(md, d, ["res", "x", "q", "adt"])
 
 
 @pytest.fixture(scope="module", params=["aos", "soa"])
