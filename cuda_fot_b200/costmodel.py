@@ -20,7 +20,7 @@ import ctypes as C
 import json
 import os
 import time
-from typing import Dict, List, Optional, Sequence
+from typing import List, Optional, Sequence
 
 import numpy as np
 

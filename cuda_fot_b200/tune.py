@@ -19,12 +19,9 @@ model's training data.
 """
 from __future__ import annotations
 
-import itertools
 import time
-from dataclasses import asdict, dataclass
+from dataclasses import dataclass
 from typing import Dict, List, Optional
-
-import numpy as np
 
 from . import fot as F
 from . import meshgen as mg

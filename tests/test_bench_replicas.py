@@ -7,8 +7,6 @@ import os
 import socket
 import sys
 
-import pytest
-
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 

@@ -8,7 +8,6 @@ and within 1e-12 (FP64) / 1e-5 (FP32 volna) of the serial loop; a CUDA graph
 of batched launches equals the same launches issued directly.  Atomic plans:
 every mesh within the same tolerances of its serial loop.
 """
-import numpy as np
 import pytest
 
 from cuda_fot_b200 import meshgen as mg

@@ -9,7 +9,6 @@ a fresh run of the same plan is again bit-identical to the CPU replay.
 """
 import time
 
-import numpy as np
 import pytest
 
 from cuda_fot_b200 import meshgen as mg
