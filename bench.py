@@ -237,7 +237,9 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--plan", default=None, help="force a candidate label order/exec/block")
+    ap.add_argument("--plan", default=None,
+                    help="force a plan by its label, order[+partN]/exec[d][-plain]/block[@soa], "
+                         "e.g. rcm/atomic-plain/256@soa")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
