@@ -1,6 +1,7 @@
 // extern "C" entry points of libfot (declared in include/fot.h).
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -157,6 +158,9 @@ fot::HierPlanDev fot_plan::dev(uint32_t iterations) const {
   P.outbuf_off = layout.outbuf_off;
   P.outbuf_bytes = layout.outbuf_bytes;
   P.block_done = block_done.as<unsigned int>();
+  P.launch = launch.as<uint32_t>();
+  P.partial = partial.ptr;
+  P.counter = counter.as<unsigned int>();
   P.ctl = ctl.as<Ctl>();
   return P;
 }
@@ -244,6 +248,9 @@ int fot_problem_create(int loop, int layout, uint32_t n_cells, const uint32_t *n
 }
 
 int fot_problem_destroy(fot_problem *p) {
+  // plans outliving their problem fail with FOT_ERR_STATE from now on
+  if (p)
+    for (fot_plan *plan : p->plans) plan->prob = nullptr;
   delete p;
   return FOT_OK;
 }
@@ -369,16 +376,21 @@ int fot_plan_build(fot_problem *p, const fot_plan_desc *desc, fot_plan **out) {
   int rc = FOT_OK;
   if (desc->exec == FOT_EXEC_ATOMIC) {
     plan->threads = 256;
-    rc = ops->occupancy(FOT_EXEC_ATOMIC, p->layout == FOT_SOA, 256, 0, 0, &plan->per_sm);
+    const uint32_t agg = (desc->flags & FOT_PLAN_NO_AGGREGATE) ? 0u : 1u;
+    rc = ops->occupancy(FOT_EXEC_ATOMIC, p->layout == FOT_SOA, 256, agg, 0, &plan->per_sm);
   } else if (desc->exec == FOT_EXEC_HIER || desc->exec == FOT_EXEC_HIER_LAUNCH) {
-    // staged reads by default; the persistent executor uses the pipelined
-    // kernel unless direct gathers or the simple tile loop are asked for
+    // staged reads by default; the persistent executor uses the split
+    // write-back kernel (or, with FOT_PLAN_BLOCK_FLAGS, the pipelined kernel
+    // with per-block completion flags) unless direct gathers or the simple
+    // tile loop are asked for
     plan->variant = (desc->flags & FOT_PLAN_DIRECT_READS) ? 0u : kVariantStage;
-    // (its two control warps need room beside the compute threads: blocks of
-    // at most 512 cells)
+    // (their two control warps need room beside the compute threads: blocks
+    // of at most 512 cells)
     if (desc->exec == FOT_EXEC_HIER && desc->block_size <= 512 &&
-        !(desc->flags & (FOT_PLAN_DIRECT_READS | FOT_PLAN_SIMPLE_TILES)))
+        !(desc->flags & (FOT_PLAN_DIRECT_READS | FOT_PLAN_SIMPLE_TILES))) {
       plan->variant |= kVariantPipe;
+      if (!(desc->flags & FOT_PLAN_BLOCK_FLAGS)) plan->variant |= kVariantSplit;
+    }
     rc = build_hier_plan(p, plan);
     if (rc == FOT_OK) {
       plan->threads = hier_threads(desc->block_size);
@@ -403,7 +415,7 @@ int fot_plan_build(fot_problem *p, const fot_plan_desc *desc, fot_plan **out) {
       // the pipelined kernel holds two tiles' rows; when they do not fit,
       // the single-buffer persistent kernel runs the plan instead
       if ((plan->variant & kVariantPipe) && plan->layout.total > 227 * 1024) {
-        plan->variant &= ~kVariantPipe;
+        plan->variant &= ~(kVariantPipe | kVariantSplit);
         ops->smem_layout(plan->cap[0], plan->cap[1], plan->variant, plan->rec_cap,
                          plan->threads, &plan->layout);
       }
@@ -447,27 +459,39 @@ int fot_plan_build(fot_problem *p, const fot_plan_desc *desc, fot_plan **out) {
                  plan->lidx[1].bytes;
   s.build_ms =
       std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  s.shared_points = plan->n_shared_points;
+  s.partial_slots = plan->n_slots;
+  const char *kname = "atomic";
+  if (desc->exec == FOT_EXEC_HIER_LAUNCH) kname = "per-colour launches";
+  else if (desc->exec == FOT_EXEC_HIER)
+    kname = (plan->variant & kVariantSplit) ? "split write-back"
+            : (plan->variant & kVariantPipe) ? "pipelined, block flags"
+            : (plan->variant & kVariantStage) ? "simple persistent"
+                                               : "simple persistent, direct reads";
+  std::snprintf(s.kernel, sizeof(s.kernel), "%s", kname);
+  p->plans.push_back(plan);
   *out = plan;
   return FOT_OK;
 }
 
 int fot_plan_destroy(fot_plan *plan) {
-  if (plan && plan->prob && plan->ctl.ptr && plan->prob->last_ctl == plan->ctl.as<Ctl>()) {
-    plan->prob->last_ctl = nullptr;
-    plan->prob->last_flags = nullptr;
-    plan->prob->last_n_blocks = 0;
+  if (plan && plan->prob) {
+    auto &v = plan->prob->pending;
+    v.erase(std::remove(v.begin(), v.end(), plan), v.end());
+    auto &w = plan->prob->plans;
+    w.erase(std::remove(w.begin(), w.end(), plan), w.end());
   }
   delete plan;
   return FOT_OK;
 }
 
-// Remember the control block and flags of the last persistent run so that
-// fot_sync can report (and clear) device-side errors.
+// Remember every plan with a device control block that ran since the last
+// fot_sync, so that fot_sync reports (and clears) the device-side errors of
+// all of them, not only of the last one.
 static void note_run(fot_problem *p, fot_plan *plan) {
   if (!plan->ctl.ptr) return;
-  p->last_ctl = plan->ctl.as<Ctl>();
-  p->last_flags = plan->block_done.ptr ? plan->block_done.as<unsigned int>() : nullptr;
-  p->last_n_blocks = plan->n_blocks;
+  if (std::find(p->pending.begin(), p->pending.end(), plan) == p->pending.end())
+    p->pending.push_back(plan);
 }
 
 int fot_plan_get_stats(const fot_plan *plan, fot_plan_stats *stats) {
@@ -482,6 +506,7 @@ int fot_plan_export(const fot_plan *plan, uint32_t *n_blocks, uint32_t *n_colour
                     uint16_t *lidx) {
   if (!plan) return fail(FOT_ERR_ARG, "null plan");
   if (plan->desc.exec == FOT_EXEC_ATOMIC) return fail(FOT_ERR_STATE, "atomic plans hold no arrays");
+  if (!plan->prob) return fail(FOT_ERR_STATE, "the plan's problem was destroyed");
   const fot_problem *p = plan->prob;
   const uint32_t nb = plan->n_blocks, n = p->n_cells;
   uint32_t total = 0;
@@ -505,7 +530,7 @@ int fot_plan_export(const fot_plan *plan, uint32_t *n_blocks, uint32_t *n_colour
 
 static int run_plan(fot_problem *p, fot_plan *plan, uint32_t iterations, cudaStream_t st) {
   if (!p || !plan) return fail(FOT_ERR_ARG, "null argument");
-  if (plan->prob != p) return fail(FOT_ERR_STATE, "plan belongs to another problem");
+  if (plan->prob != p) return fail(FOT_ERR_STATE, "plan belongs to another (or a destroyed) problem");
   if (iterations == 0) return FOT_OK;
   const LoopOps *ops = loop_ops(p->loop);
   const LoopData d = p->loop_data();
@@ -524,7 +549,9 @@ static int run_plan(fot_problem *p, fot_plan *plan, uint32_t iterations, cudaStr
     if ((uint64_t)iterations * plan->n_blocks + (uint64_t)plan->per_sm * sms >= 0xFFFFFFFFull)
       return fail(FOT_ERR_LIMIT, "too many tiles in one launch");
     const HierPlanDev P = plan->dev(iterations);
-    const uint32_t grid = std::min<uint32_t>(P.total_tiles, (uint32_t)(plan->per_sm * sms));
+    // the split kernel runs one iteration per launch over the plan's blocks
+    const uint32_t tiles = (plan->variant & kVariantSplit) ? plan->n_blocks : P.total_tiles;
+    const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)(plan->per_sm * sms));
     return ops->run_hier(d, P, soa, plan->threads, plan->variant, grid, plan->smem, st);
   }
   const HierPlanDev P = plan->dev(1);
@@ -548,16 +575,23 @@ int fot_run(fot_problem *p, fot_plan *plan, uint32_t iterations, void *stream) {
 int fot_sync(fot_problem *p, void *stream) {
   if (!p) return fail(FOT_ERR_ARG, "null problem");
   FOT_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
-  if (p->last_ctl) {
+  std::vector<fot_plan *> pending;
+  pending.swap(p->pending);
+  int failed = 0;
+  for (fot_plan *plan : pending) {
     Ctl c{};
-    FOT_CUDA(cudaMemcpy(&c, p->last_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
-    if (c.error) {
-      // the run stopped early: restart the plan's queue and flags from zero
-      FOT_CUDA(cudaMemset(p->last_ctl, 0, sizeof(Ctl)));
-      if (p->last_flags) FOT_CUDA(cudaMemset(p->last_flags, 0, (size_t)p->last_n_blocks * 4));
-      return fail(FOT_ERR_DEVICE, "a dependency wait of the persistent executor hit its limit");
-    }
+    FOT_CUDA(cudaMemcpy(&c, plan->ctl.ptr, sizeof(Ctl), cudaMemcpyDeviceToHost));
+    if (!c.error) continue;
+    // the run stopped early: restart the plan's queue, flags and arrival
+    // counters from zero
+    ++failed;
+    FOT_CUDA(cudaMemset(plan->ctl.ptr, 0, sizeof(Ctl)));
+    if (plan->block_done.ptr) FOT_CUDA(cudaMemset(plan->block_done.ptr, 0, (size_t)plan->n_blocks * 4));
+    if (plan->counter.ptr) FOT_CUDA(cudaMemset(plan->counter.ptr, 0, (size_t)plan->n_slots * 4));
   }
+  if (failed)
+    return fail(FOT_ERR_DEVICE, "%d hierarchical plan(s) stopped early: a wait of the persistent "
+                "executor hit its limit (the problem's data are undefined)", failed);
   return FOT_OK;
 }
 

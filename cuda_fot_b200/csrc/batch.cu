@@ -5,7 +5,8 @@
 //     different sizes share the GPU without a launch per mesh and colour;
 //   * atomic plans: tiles of 1,024 consecutive cells of one mesh, for every
 //     mesh and every iteration, in one grid-stride launch (iterations need no
-//     ordering: the loops never read the dataset they increment).
+//     ordering: the loops never read the dataset they increment); that
+//     kernel lives in atomic_batch.cu.
 // The reference has no counterpart (one mesh per process, one launch per
 // colour).
 #define FOT_ADAPTER_ALL 1
@@ -13,27 +14,11 @@
 #include <numeric>
 
 #include "devutil.cuh"
+#include "batch.cuh"
 #include "engine.hpp"
 #include "loops.cuh"
 
 namespace fot {
-
-struct BatchMesh {
-  LoopData d;
-  HierPlanDev P;
-  int loop;
-};
-
-struct BatchDev {
-  const BatchMesh *mesh;
-  const uint32_t *tile_mesh;  // per tile of one iteration: mesh index
-  const uint32_t *tile_block; // per tile: block of that mesh
-  uint32_t tiles_per_iter;
-  uint32_t total_tiles;
-  uint32_t n_mesh;
-  unsigned int *done; // per mesh
-  Ctl *ctl;           // ticket / exited / error
-};
 
 template <bool SOA, int T, class L>
 __device__ __forceinline__ void batch_tile(const BatchMesh &m, unsigned char *smem, uint32_t b,
@@ -76,54 +61,6 @@ __global__ void __launch_bounds__(T) k_batch(BatchDev B) {
       __threadfence();
     }
   }
-}
-
-constexpr uint32_t kAtomicTile = 1024;  // cells per tile of the atomic batch
-
-template <class... Ls> constexpr int max_reg_cap() {
-  int m = 0;
-  ((m = Ls::kRegCap > m ? Ls::kRegCap : m), ...);
-  return m;
-}
-
-template <bool SOA, bool AGG, class... Ls>
-__global__ void __launch_bounds__(256, (65536 / (256 * max_reg_cap<Ls...>())) > 0
-                                           ? 65536 / (256 * max_reg_cap<Ls...>()) : 1)
-    k_batch_atomic(BatchDev B) {
-  const uint32_t warp = threadIdx.x >> 5;
-  for (uint32_t t = blockIdx.x; t < B.total_tiles; t += gridDim.x) {
-    const uint32_t r = t % B.tiles_per_iter;
-    const BatchMesh &m = B.mesh[B.tile_mesh[r]];
-    const uint32_t start = B.tile_block[r];
-#pragma unroll 1
-    for (uint32_t k = 0; k < kAtomicTile / 256; ++k) {
-      const uint32_t base = start + (k * 8u + warp) * 32u;
-      ((m.loop == Ls::kLoop ? (atomic_warp<Ls, SOA, AGG>(m.d, base), 0) : 0), ...);
-    }
-  }
-}
-
-template <bool SOA, bool AGG> const void *batch_atomic_kernel(uint32_t loop_mask) {
-  using RC = res_calc::Loop;
-  using MA = mini_aero::Loop;
-  using LU = lulesh::Loop;
-  using VO = volna::Loop;
-  using GA = getacc::Loop;
-  switch (loop_mask) {
-  case 1u << FOT_LOOP_RES_CALC: return (const void *)&k_batch_atomic<SOA, AGG, RC>;
-  case 1u << FOT_LOOP_MINI_AERO: return (const void *)&k_batch_atomic<SOA, AGG, MA>;
-  case 1u << FOT_LOOP_LULESH: return (const void *)&k_batch_atomic<SOA, AGG, LU>;
-  case 1u << FOT_LOOP_VOLNA: return (const void *)&k_batch_atomic<SOA, AGG, VO>;
-  case 1u << FOT_LOOP_GETACC: return (const void *)&k_batch_atomic<SOA, AGG, GA>;
-  case (1u << FOT_LOOP_RES_CALC) | (1u << FOT_LOOP_VOLNA):
-    return (const void *)&k_batch_atomic<SOA, AGG, RC, VO>;
-  }
-  return nullptr;
-}
-
-const void *batch_atomic_kernel_for(bool soa, bool agg, uint32_t loop_mask) {
-  if (soa) return agg ? batch_atomic_kernel<true, true>(loop_mask) : batch_atomic_kernel<true, false>(loop_mask);
-  return agg ? batch_atomic_kernel<false, true>(loop_mask) : batch_atomic_kernel<false, false>(loop_mask);
 }
 
 // Kernel variants: one loop kind, or the res_calc + volna pair.

@@ -30,8 +30,10 @@ struct SmemLayout {
 // pipelined persistent kernel (warp-specialised: tile records by bulk copy,
 // double-buffered staging, per-point gather of the increments), launched
 // with 64 threads more than `threads` for its two control warps; bit 2 = that
-// kernel with three tile-record slots (else two).
-constexpr uint32_t kVariantStage = 1u, kVariantPipe = 2u, kVariantSlots3 = 4u;
+// kernel with three tile-record slots (else two); bit 3 = the split
+// write-back kernel (hier_split.cuh; with bit 1, same control warps and slot
+// counts, one launch per iteration).
+constexpr uint32_t kVariantStage = 1u, kVariantPipe = 2u, kVariantSlots3 = 4u, kVariantSplit = 8u;
 
 struct LoopOps {
   // launch one iteration of the atomic executor
@@ -87,9 +89,10 @@ struct fot_problem {
   std::vector<uint32_t> partition;     // part of each cell (current order), may be empty
   uint64_t version = 1; // bumped whenever cells or points are renumbered
   int device = 0;
-  fot::Ctl *last_ctl = nullptr; // control block of the last persistent run
-  unsigned int *last_flags = nullptr; // its per-block completion flags
-  uint32_t last_n_blocks = 0;
+  // plans with a device control block run since the last fot_sync
+  std::vector<struct fot_plan *> pending;
+  // live plans built on this problem (told when the problem is destroyed)
+  std::vector<struct fot_plan *> plans;
 
   size_t point_bytes(uint32_t k) const {
     return (size_t)n_points[k] * info.point_dim[k] * info.point_type_size[k];
@@ -116,6 +119,9 @@ struct fot_plan {
   fot::DevBuf build_perm; // position -> cell index before the build
   fot::DevBuf rec, rec_off; // tile records (see plan.cu)
   fot::DevBuf block_done;   // per block: completed iterations (pipelined executor)
+  // split write-back kernel: partial-sum slots, arrival counters, tile order
+  fot::DevBuf partial, counter, launch;
+  uint32_t n_slots = 0, n_shared_points = 0;
   uint32_t rec_cap = 0;
   uint32_t cap[2] = {0, 0};
   fot::SmemLayout layout;

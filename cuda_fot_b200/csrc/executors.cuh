@@ -25,8 +25,12 @@
 //     with has been written back: every tile of the earlier colours for the
 //     simple kernel (k_hier, hier.cuh), the conflicting blocks' completion
 //     flags for the pipelined warp-specialised kernel (k_hier_pipe,
-//     hier_pipe.cuh, the default).  The result is therefore deterministic
-//     and equal to replaying the colours in order on the CPU.
+//     hier_pipe.cuh).  The split write-back kernel (k_hier_split,
+//     hier_split.cuh, the default) makes no tile wait: points written by one
+//     block are added at once, points shared by several blocks through
+//     per-block partial sums that the last block to arrive adds in colour
+//     order.  The result is therefore deterministic and equal to replaying
+//     the colours in order on the CPU.
 #pragma once
 
 #include <cstdint>
@@ -70,6 +74,10 @@ struct HierPlanDev {
   uint32_t outbuf_off;         // first prefetched-output-row slot
   uint32_t outbuf_bytes;       // bytes of one output-row slot
   unsigned int *block_done;    // per block: completed iterations (relative to ctl->base)
+  // split write-back kernel
+  const uint32_t *launch;      // tile -> block (formation order)
+  void *partial;               // partial-sum slots (AOS rows of point dataset 0's type)
+  unsigned int *counter;       // arrivals per shared point (at its first slot)
 };
 
 // Direct (cell) data of one cell: SOA with stride n_cells.
@@ -239,3 +247,4 @@ __global__ void __launch_bounds__(256, (65536 / (256 * L::kRegCap)) > 0 ? 65536 
 
 #include "hier.cuh"
 #include "hier_pipe.cuh"
+#include "hier_split.cuh"

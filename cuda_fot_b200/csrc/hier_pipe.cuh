@@ -241,6 +241,7 @@ __global__ void __launch_bounds__(T + 64) __maxnreg__(L::kRegCap)
   __shared__ uint32_t s_iter[kRecSlots];   // iteration of the tile in each record slot
   __shared__ uint32_t s_valid[kRecSlots];  // 0: no tile (end of this CTA's queue)
   __shared__ uint32_t s_abort[2];          // per row slot: skip the write-back
+  __shared__ uint32_t s_tile_abort[kRecSlots];  // per record slot: the tile was not written back
   __shared__ volatile uint32_t s_stop;     // a role gave up (error path)
   const uint32_t tid = threadIdx.x;
   const uint32_t warp = tid >> 5, lane = tid & 31u;
@@ -301,6 +302,12 @@ __global__ void __launch_bounds__(T + 64) __maxnreg__(L::kRegCap)
         if (!valid[s]) break;
         if (!mbar_wait_or_stop(&s_tile_done[s], (j / kRecSlots) & 1u, &s_stop)) {
           atomicOr(&P.ctl->error, kErrWaitLimit);
+          s_stop = 1;
+          break;
+        }
+        // a tile that skipped its write-back publishes no completion: its
+        // dependents time out instead of adding on top of missing sums
+        if (s_tile_abort[s]) {
           s_stop = 1;
           break;
         }
@@ -448,6 +455,7 @@ __global__ void __launch_bounds__(T + 64) __maxnreg__(L::kRegCap)
           }
         }
       }
+      if (tid == 0) s_tile_abort[s] = (ok_out && !s_abort[b]) ? 0u : 1u;
       __syncwarp();
       if (lane == 0) mbar_arrive(&s_tile_done[s]);
       // the increments buffer is reused by the next tile

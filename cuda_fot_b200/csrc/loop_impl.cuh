@@ -1,30 +1,23 @@
-// Instantiates both executors for the loop selected by FOT_ADAPTER and
-// exposes them through a LoopOps table.  Included once by each loop_*.cu.
+// Instantiates the hierarchical-colour executors for the loop selected by
+// FOT_ADAPTER and exposes them, with the atomic executor of the loop's
+// atomic_*.cu unit, through a LoopOps table.  Included once by each
+// loop_*.cu (compiled without multiply-add contraction: coloured runs are
+// bit-identical to their CPU replay).
 #pragma once
 
 #include "engine.hpp"
 #include "loops.cuh"
 
 namespace fot {
+
+// the atomic executor of this loop (atomic_*.cu, loop_atomic_impl.cuh)
+int FOT_CAT(atomic_run_, FOT_ADAPTER_NS)(const LoopData &d, bool soa, bool agg, uint32_t threads,
+                                         uint32_t grid, cudaStream_t st);
+int FOT_CAT(atomic_occupancy_, FOT_ADAPTER_NS)(bool soa, bool agg, int *per_sm);
+
 namespace FOT_ADAPTER_NS {
 
 using L = Loop;
-
-template <bool SOA, bool AGG> int launch_atomic(const LoopData &d, uint32_t threads,
-                                               uint32_t grid, cudaStream_t st) {
-  if (threads != 256) return fail(FOT_ERR_ARG, "atomic executor runs 256 threads per CTA");
-  k_atomic<L, SOA, AGG><<<grid, 256, 0, st>>>(d);
-  FOT_CUDA(cudaGetLastError());
-  return FOT_OK;
-}
-
-int run_atomic(const LoopData &d, bool soa, bool agg, uint32_t threads, uint32_t grid,
-               cudaStream_t st) {
-  if (soa) return agg ? launch_atomic<true, true>(d, threads, grid, st)
-                      : launch_atomic<true, false>(d, threads, grid, st);
-  return agg ? launch_atomic<false, true>(d, threads, grid, st)
-             : launch_atomic<false, false>(d, threads, grid, st);
-}
 
 template <bool SOA, int T, bool STAGE> const void *hier_kernel(bool persistent) {
   return persistent ? reinterpret_cast<const void *>(&k_hier<L, SOA, T, STAGE>)
@@ -50,11 +43,23 @@ template <bool SOA, uint32_t SLOTS> const void *pipe_kernel(uint32_t threads) {
   return nullptr;
 }
 
-// variant: kVariantStage (staged reads), kVariantPipe (pipelined kernel)
+template <bool SOA, uint32_t SLOTS> const void *split_kernel(uint32_t threads) {
+  switch (threads) {
+  case 128: return reinterpret_cast<const void *>(&k_hier_split<L, SOA, 128, SLOTS>);
+  case 256: return reinterpret_cast<const void *>(&k_hier_split<L, SOA, 256, SLOTS>);
+  case 512: return reinterpret_cast<const void *>(&k_hier_split<L, SOA, 512, SLOTS>);
+  }
+  return nullptr;
+}
+
+// variant: kVariantStage (staged reads), kVariantPipe (pipelined kernel),
+// kVariantSplit (split write-back kernel)
 const void *kernel_for(int exec, bool soa, uint32_t threads, uint32_t variant) {
-  if (exec == FOT_EXEC_ATOMIC)
-    return soa ? reinterpret_cast<const void *>(&k_atomic<L, true, true>)
-               : reinterpret_cast<const void *>(&k_atomic<L, false, true>);
+  if (exec == FOT_EXEC_ATOMIC) return nullptr;
+  if (exec == FOT_EXEC_HIER && (variant & kVariantSplit)) {
+    if (variant & kVariantSlots3) return soa ? split_kernel<true, 3>(threads) : split_kernel<false, 3>(threads);
+    return soa ? split_kernel<true, 2>(threads) : split_kernel<false, 2>(threads);
+  }
   if (exec == FOT_EXEC_HIER && (variant & kVariantPipe)) {
     if (variant & kVariantSlots3) return soa ? pipe_kernel<true, 3>(threads) : pipe_kernel<false, 3>(threads);
     return soa ? pipe_kernel<true, 2>(threads) : pipe_kernel<false, 2>(threads);
@@ -79,6 +84,28 @@ int run_hier(const LoopData &d, const HierPlanDev &P, bool soa, uint32_t threads
   FOT_TRY(prepare(k, smem));
   void *args[] = {const_cast<LoopData *>(&d), const_cast<HierPlanDev *>(&P)};
   const uint32_t block = (variant & kVariantPipe) ? threads + 64 : threads;
+  if (variant & kVariantSplit) {
+    // one launch per iteration; from the second on, programmatic dependent
+    // launch lets the next iteration's tiles stage and compute while this
+    // one drains (the kernel waits before it writes).  The first launch of
+    // a call is fully stream-ordered: whatever precedes it may write the
+    // datasets it reads.
+    const uint32_t iters = P.n_blocks ? P.total_tiles / P.n_blocks : 0;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    for (uint32_t it = 0; it < iters; ++it) {
+      cfg.attrs = it > 0 ? attr : nullptr;
+      cfg.numAttrs = it > 0 ? 1 : 0;
+      FOT_CUDA(cudaLaunchKernelExC(&cfg, k, args));
+    }
+    return FOT_OK;
+  }
   FOT_CUDA(cudaLaunchKernel(k, dim3(grid), dim3(block), args, smem, st));
   return FOT_OK;
 }
@@ -95,10 +122,13 @@ int run_hier_colour(const LoopData &d, const HierPlanDev &P, bool soa, uint32_t 
 }
 
 int occupancy(int exec, bool soa, uint32_t threads, uint32_t variant, size_t smem, int *per_sm) {
-  const void *k = kernel_for(exec, soa, exec == FOT_EXEC_ATOMIC ? 256 : threads, variant);
+  // atomic plans: `variant` bit 0 set = warp aggregation
+  if (exec == FOT_EXEC_ATOMIC)
+    return FOT_CAT(atomic_occupancy_, FOT_ADAPTER_NS)(soa, variant & 1u, per_sm);
+  const void *k = kernel_for(exec, soa, threads, variant);
   if (!k) return fail(FOT_ERR_ARG, "no kernel for %u threads", threads);
-  if (exec != FOT_EXEC_ATOMIC) FOT_TRY(prepare(k, smem));
-  int block = exec == FOT_EXEC_ATOMIC ? 256 : (int)threads;
+  FOT_TRY(prepare(k, smem));
+  int block = (int)threads;
   if (exec == FOT_EXEC_HIER && (variant & kVariantPipe)) block += 64;
   FOT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k, block, smem));
   return FOT_OK;
@@ -114,7 +144,8 @@ void smem_layout(uint32_t cap0, uint32_t cap1, uint32_t variant, uint32_t rec_ca
   size_t off = 0;
   if (variant & kVariantPipe) {
     // 2 or 3 tile-record slots, 2 read-row slots, the per-slot increments, 2
-    // prefetched-output-row slots (AOS output rows of a multiple of 16 bytes)
+    // prefetched-output-row slots (AOS output rows of a multiple of 16 bytes;
+    // not in the split write-back kernel)
     auto a128 = [](size_t v) { return (v + 127) & ~size_t(127); };
     s.rec_slot = (uint32_t)a128(rec_cap);
     off = ((variant & kVariantSlots3) ? 3 : 2) * (size_t)s.rec_slot;
@@ -130,7 +161,7 @@ void smem_layout(uint32_t cap0, uint32_t cap1, uint32_t variant, uint32_t rec_ca
     s.inc_off = (uint32_t)off;
     off = a128(off + (size_t)L::kOut * L::kDim * threads * sizeof(out_t));
     s.outbuf_off = (uint32_t)off;
-    if ((L::kOut * sizeof(out_t)) % 16 == 0) {
+    if (!(variant & kVariantSplit) && (L::kOut * sizeof(out_t)) % 16 == 0) {
       s.outbuf_bytes = (uint32_t)a128((size_t)cap0 * L::kOut * sizeof(out_t));
       off += 2 * (size_t)s.outbuf_bytes;
     }
@@ -156,7 +187,7 @@ void smem_layout(uint32_t cap0, uint32_t cap1, uint32_t variant, uint32_t rec_ca
 } // namespace FOT_ADAPTER_NS
 
 extern const LoopOps FOT_OPS_NAME;
-const LoopOps FOT_OPS_NAME = {FOT_ADAPTER_NS::run_atomic, FOT_ADAPTER_NS::run_hier,
+const LoopOps FOT_OPS_NAME = {FOT_CAT(atomic_run_, FOT_ADAPTER_NS), FOT_ADAPTER_NS::run_hier,
                               FOT_ADAPTER_NS::run_hier_colour, FOT_ADAPTER_NS::occupancy,
                               FOT_ADAPTER_NS::smem_layout};
 } // namespace fot

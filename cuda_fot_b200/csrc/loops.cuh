@@ -11,6 +11,7 @@
 //                 mapping class (0: mapping 0; 1: a second, distinct mapping
 //                 such as res_calc's edge->node), dimension, element type
 //   direct sets   cell datasets (SOA), element type, and which are written
+//                 (kWritesCell: the cell function writes a cell dataset)
 // and a device function cell() that, given row pointers of the read sets for
 // each slot (in global memory or staged in shared memory) and the cell's
 // direct data, produces the signed per-slot increments inc[slot][k] such that
@@ -41,6 +42,17 @@
 #ifndef FOT_FUNCTOR_DIR
 #define FOT_FUNCTOR_DIR kernels
 #endif
+// Namespace of a loop's adapter and functor: the loop's name, plus
+// FOT_NS_SUFFIX when a translation unit defines it (the atomic executor's
+// units, compiled with multiply-add contraction, instantiate the same
+// functors under res_calc_fma, ... so that their symbols stay apart from the
+// exact instantiations of the coloured executors).
+#ifndef FOT_NS_SUFFIX
+#define FOT_NS_SUFFIX
+#endif
+#define FOT_CAT2(a, b) a##b
+#define FOT_CAT(a, b) FOT_CAT2(a, b)
+#define FOT_LNS(name) FOT_CAT(name, FOT_NS_SUFFIX)
 #define FOT_STR2(x) #x
 #define FOT_STR(x) FOT_STR2(x)
 #define FOT_FUNCTOR(file) FOT_STR(FOT_FUNCTOR_DIR/file)
@@ -52,7 +64,7 @@ namespace fot {
 // adt through the edge->cell mapping (res_calc.hpp:29-89).
 // --------------------------------------------------------------------------
 #if FOT_ADAPTER == FOT_LOOP_RES_CALC || defined(FOT_ADAPTER_ALL)
-namespace res_calc {
+namespace FOT_LNS(res_calc) {
 #define USER_FUNCTION_SIGNATURE __device__ __forceinline__ void user_func_gpu
 #define RESTRICT __restrict__
 #include FOT_FUNCTOR(res_calc_func.hpp)
@@ -71,6 +83,7 @@ struct Loop {
   __host__ __device__ static constexpr int read_class(int r) { return r == 0 ? 1 : 0; }
   __host__ __device__ static constexpr int read_dim(int r) { return r == 0 ? 2 : (r == 1 ? 4 : 1); }
   static constexpr int kNumDirect = 0;
+  static constexpr bool kWritesCell = false; // no cell dataset is written
 
   template <class Rows, class Direct>
   __device__ __forceinline__ static void cell(const Rows &rows, const Direct &,
@@ -89,7 +102,7 @@ struct Loop {
 // record is direct data; left -= flux, right += flux (mini_aero.hpp:43-111).
 // --------------------------------------------------------------------------
 #if FOT_ADAPTER == FOT_LOOP_MINI_AERO || defined(FOT_ADAPTER_ALL)
-namespace mini_aero {
+namespace FOT_LNS(mini_aero) {
 #define USER_FUNCTION_SIGNATURE __device__ __forceinline__ void user_func_gpu
 #define RESTRICT __restrict__
 #include FOT_FUNCTOR(mini_aero_func.hpp)
@@ -107,6 +120,7 @@ struct Loop {
   __host__ __device__ static constexpr int read_class(int) { return 0; }
   __host__ __device__ static constexpr int read_dim(int) { return 28; }
   static constexpr int kNumDirect = 1;
+  static constexpr bool kWritesCell = false;
 
   template <class Rows, class Direct>
   __device__ __forceinline__ static void cell(const Rows &rows, const Direct &dir,
@@ -135,7 +149,7 @@ struct Loop {
 // the direct dataset determ (lulesh.hpp:23-58).
 // --------------------------------------------------------------------------
 #if FOT_ADAPTER == FOT_LOOP_LULESH || defined(FOT_ADAPTER_ALL)
-namespace lulesh {
+namespace FOT_LNS(lulesh) {
 static constexpr unsigned MESH_DIM = 8;
 #define USER_FUNCTION_SIGNATURE __device__ __forceinline__ void user_func_gpu
 #define RESTRICT __restrict__
@@ -154,6 +168,7 @@ struct Loop {
   __host__ __device__ static constexpr int read_class(int) { return 0; }
   __host__ __device__ static constexpr int read_dim(int) { return 3; }
   static constexpr int kNumDirect = 2;
+  static constexpr bool kWritesCell = true; // determ (cell dataset 1)
 
   template <class Rows, class Direct>
   __device__ __forceinline__ static void cell(const Rows &rows, const Direct &dir,
@@ -181,7 +196,7 @@ struct Loop {
 // (volna.hpp:30-75).
 // --------------------------------------------------------------------------
 #if FOT_ADAPTER == FOT_LOOP_VOLNA || defined(FOT_ADAPTER_ALL)
-namespace volna {
+namespace FOT_LNS(volna) {
 #define USER_FUNCTION_SIGNATURE __device__ __forceinline__ void user_func_gpu
 #define RESTRICT __restrict__
 #include FOT_FUNCTOR(volna_func.hpp)
@@ -199,6 +214,7 @@ struct Loop {
   __host__ __device__ static constexpr int read_class(int) { return 0; }
   __host__ __device__ static constexpr int read_dim(int) { return 1; }
   static constexpr int kNumDirect = 4;
+  static constexpr bool kWritesCell = false;
 
   template <class Rows, class Direct>
   __device__ __forceinline__ static void cell(const Rows &rows, const Direct &dir,
@@ -220,7 +236,7 @@ struct Loop {
 // (getacc_scatter.hpp:29-75).
 // --------------------------------------------------------------------------
 #if FOT_ADAPTER == FOT_LOOP_GETACC || defined(FOT_ADAPTER_ALL)
-namespace getacc {
+namespace FOT_LNS(getacc) {
 #define USER_FUNCTION_SIGNATURE __device__ __forceinline__ void user_func_gpu
 #define RESTRICT __restrict__
 #include FOT_FUNCTOR(getacc_scatter_func.hpp)
@@ -238,6 +254,7 @@ struct Loop {
   __host__ __device__ static constexpr int read_class(int) { return 0; }
   __host__ __device__ static constexpr int read_dim(int) { return 1; }
   static constexpr int kNumDirect = 5;
+  static constexpr bool kWritesCell = false;
 
   template <class Rows, class Direct>
   __device__ __forceinline__ static void cell(const Rows &, const Direct &dir,

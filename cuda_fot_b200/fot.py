@@ -32,6 +32,7 @@ AOS, SOA = 0, 1
 EXEC_ATOMIC, EXEC_HIER, EXEC_HIER_LAUNCH = 0, 1, 2
 ORDER_NATURAL, ORDER_RANDOM, ORDER_RCM, ORDER_GPS = 0, 1, 2, 3
 PLAN_NO_AGGREGATE, PLAN_USE_PARTITION, PLAN_DIRECT_READS, PLAN_SIMPLE_TILES = 1, 2, 4, 8
+PLAN_BLOCK_FLAGS = 16
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(f"{LIB_PATH} is missing: build it with `python -m cuda_fot_b200.build`")
@@ -72,10 +73,13 @@ class PlanStats(C.Structure):
                 ("max_block_points1", C.c_uint32), ("max_thread_colours", C.c_uint32),
                 ("avg_thread_colours", C.c_double), ("avg_block_points", C.c_double),
                 ("plan_bytes", C.c_uint64), ("smem_bytes", C.c_uint32), ("grid", C.c_uint32),
-                ("build_ms", C.c_double)]
+                ("build_ms", C.c_double), ("shared_points", C.c_uint32),
+                ("partial_slots", C.c_uint32), ("kernel", C.c_char * 32)]
 
     def as_dict(self):
-        return {name: getattr(self, name) for name, _ in self._fields_}
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["kernel"] = d["kernel"].decode()
+        return d
 
 
 def version() -> str:

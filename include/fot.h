@@ -78,6 +78,13 @@ extern "C" {
                                      staging them in shared memory */
 #define FOT_PLAN_SIMPLE_TILES 8u  /* persistent hierarchical: one tile at a time with a
                                      barrier per thread colour (no pipelining) */
+#define FOT_PLAN_BLOCK_FLAGS 16u  /* persistent hierarchical: the pipelined kernel whose tiles
+                                     wait for the per-block completion flags of the blocks
+                                     they conflict with, all iterations in one launch (the
+                                     default is the split write-back kernel: no tile waits,
+                                     points shared by several blocks are summed in colour
+                                     order by the last block to arrive, one launch per
+                                     iteration) */
 
 typedef struct fot_problem fot_problem;
 typedef struct fot_plan fot_plan;
@@ -195,6 +202,9 @@ typedef struct fot_plan_stats {
   uint32_t smem_bytes;         /* dynamic shared memory per CTA */
   uint32_t grid;               /* CTAs per launch */
   double build_ms;             /* wall time of fot_plan_build */
+  uint32_t shared_points;      /* split write-back: points written by more than one block */
+  uint32_t partial_slots;      /* split write-back: (shared point, block) partial-sum slots */
+  char kernel[32];             /* the kernel form that runs the plan */
 } fot_plan_stats;
 
 /* Build an execution plan on the GPU.  For the hierarchical executors this

@@ -30,11 +30,10 @@ def build_oracle() -> None:
 
 
 def build_ref() -> bool:
-    """Compile the reference's serial path where its sources exist."""
-    if not os.path.isdir("/root/reference"):
-        return False
-    subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
-    return True
+    """Compile the reference's serial path where its sources exist (REF_DIR
+    in the environment, else oracle/Makefile's default)."""
+    subprocess.run(["make", "-s", "-C", HERE, "ref-if-present"], check=True)
+    return os.path.exists(os.path.join(HERE, "_ref", "libref.so"))
 
 
 _orc = None

@@ -61,7 +61,8 @@ def test_atomic_matches_serial(loop, layout, aggregate):
 
 
 KERNELS = {  # executor, plan flags
-    "pipelined": (1, 0), "simple": (1, 8), "direct": (1, 4), "per_colour": (2, 0),
+    "split": (1, 0), "pipelined": (1, 16), "simple": (1, 8), "direct": (1, 4),
+    "per_colour": (2, 0),
 }
 
 
@@ -156,3 +157,28 @@ def test_benchmark_sizes_against_serial(loop, gen):
     ph = F().Problem.from_mesh(md)
     ph.loop_gpu_hierarchical(1, 256)
     assert rel_err(ph.point_weights(0), ser[0]) <= 1e-12
+
+
+@pytest.mark.parametrize("loop", range(5))
+@pytest.mark.parametrize("layout", ["aos", "soa"])
+def test_split_writeback_repeated_launches_match_replay(loop, layout):
+    """The split write-back kernel runs one launch per iteration and resets
+    its arrival counters itself: one call of 4 iterations (chained launches)
+    and 4 calls of 1 iteration both equal the CPU replay of 4 iterations, and
+    the plan has points shared by several blocks to exercise the combine."""
+    md = medium(loop, layout)
+    outs = []
+    for calls in ((4,), (1, 1, 1, 1)):
+        p = F().Problem.from_mesh(md)
+        plan = p.plan(F().EXEC_HIER, 64)
+        st = plan.stats()
+        assert st["kernel"] == "split write-back"
+        assert st["shared_points"] > 0 and st["partial_slots"] > st["shared_points"]
+        ex = plan.export()
+        for k in calls:
+            plan.run(k)
+        p.sync()
+        outs.append(p.point_weights(0))
+    rep, _ = O.replay_hier(md, ex, 4)
+    assert bitwise_equal(outs[0], rep[0])
+    assert bitwise_equal(outs[1], rep[0])

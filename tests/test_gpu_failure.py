@@ -26,7 +26,7 @@ def F():
 def test_lost_completion_flag_is_reported_and_recovered():
     md = mg.res_calc(64, 48, 5)
     p = F().Problem.from_mesh(md)
-    plan = p.plan(F().EXEC_HIER, 128)
+    plan = p.plan(F().EXEC_HIER, 128, F().PLAN_BLOCK_FLAGS)
     ex = plan.export()
     with pytest.raises(F().FotError) as e:
         plan.inject_lost_flag(0)  # nothing has run yet
@@ -52,7 +52,7 @@ def test_lost_completion_flag_is_reported_and_recovered():
 def test_other_work_runs_after_a_failed_run():
     md = mg.volna(40, 30, 6)
     p = F().Problem.from_mesh(md)
-    plan = p.plan(F().EXEC_HIER, 64)
+    plan = p.plan(F().EXEC_HIER, 64, F().PLAN_BLOCK_FLAGS)
     plan.run(1)
     p.sync()
     plan.inject_lost_flag(0)
@@ -68,3 +68,23 @@ def test_other_work_runs_after_a_failed_run():
     p2.sync()
     rep, _ = O.replay_hier(md2, ex2, 2)
     assert bitwise_equal(p2.point_weights(0), rep[0])
+
+
+def test_sync_reports_an_earlier_plans_failure_once():
+    """fot_sync checks every plan run since the previous sync, not only the
+    last one: a failed hierarchical run followed by an atomic run on the same
+    problem is still reported, and the next sync is clean."""
+    md = mg.res_calc(64, 48, 9)
+    p = F().Problem.from_mesh(md)
+    bad = p.plan(F().EXEC_HIER, 128, F().PLAN_BLOCK_FLAGS)
+    n_blocks = bad.export()["n_blocks"]
+    bad.run(1)
+    p.sync()
+    bad.inject_lost_flag(n_blocks // 3)
+    bad.run(1)
+    atomic = p.plan(F().EXEC_ATOMIC, 256)
+    atomic.run(1)
+    with pytest.raises(F().FotError) as e:
+        p.sync()
+    assert e.value.code == -5
+    p.sync()  # reported once; the plan was reset
