@@ -160,7 +160,11 @@ fot::HierPlanDev fot_plan::dev(uint32_t iterations) const {
   P.block_done = block_done.as<unsigned int>();
   P.launch = launch.as<uint32_t>();
   P.partial = partial.ptr;
-  P.counter = counter.as<unsigned int>();
+  P.comb_point = comb_point.as<uint32_t>();
+  P.comb_base = comb_base.as<uint32_t>();
+  P.n_slots = n_slots;
+  P.n_shared = n_shared_points;
+  P.tiles_on = 1;
   P.ctl = ctl.as<Ctl>();
   return P;
 }
@@ -379,17 +383,17 @@ int fot_plan_build(fot_problem *p, const fot_plan_desc *desc, fot_plan **out) {
     const uint32_t agg = (desc->flags & FOT_PLAN_NO_AGGREGATE) ? 0u : 1u;
     rc = ops->occupancy(FOT_EXEC_ATOMIC, p->layout == FOT_SOA, 256, agg, 0, &plan->per_sm);
   } else if (desc->exec == FOT_EXEC_HIER || desc->exec == FOT_EXEC_HIER_LAUNCH) {
-    // staged reads by default; the persistent executor uses the split
-    // write-back kernel (or, with FOT_PLAN_BLOCK_FLAGS, the pipelined kernel
-    // with per-block completion flags) unless direct gathers or the simple
-    // tile loop are asked for
-    plan->variant = (desc->flags & FOT_PLAN_DIRECT_READS) ? 0u : kVariantStage;
-    // (their two control warps need room beside the compute threads: blocks
-    // of at most 512 cells)
+    // Persistent executor (blocks of at most 512 cells): the staged split
+    // write-back kernel by default, the direct split write-back kernel with
+    // FOT_PLAN_DIRECT_READS, the pipelined kernel with per-block completion
+    // flags with FOT_PLAN_BLOCK_FLAGS; FOT_PLAN_SIMPLE_TILES (or larger
+    // blocks) selects the simple persistent kernel, staged or direct.
+    const bool direct = desc->flags & FOT_PLAN_DIRECT_READS;
+    plan->variant = direct ? 0u : kVariantStage;
     if (desc->exec == FOT_EXEC_HIER && desc->block_size <= 512 &&
-        !(desc->flags & (FOT_PLAN_DIRECT_READS | FOT_PLAN_SIMPLE_TILES))) {
-      plan->variant |= kVariantPipe;
-      if (!(desc->flags & FOT_PLAN_BLOCK_FLAGS)) plan->variant |= kVariantSplit;
+        !(desc->flags & FOT_PLAN_SIMPLE_TILES)) {
+      if (direct) plan->variant |= kVariantSplit;
+      else plan->variant |= kVariantPipe | ((desc->flags & FOT_PLAN_BLOCK_FLAGS) ? 0u : kVariantSplit);
     }
     rc = build_hier_plan(p, plan);
     if (rc == FOT_OK) {
@@ -464,7 +468,8 @@ int fot_plan_build(fot_problem *p, const fot_plan_desc *desc, fot_plan **out) {
   const char *kname = "atomic";
   if (desc->exec == FOT_EXEC_HIER_LAUNCH) kname = "per-colour launches";
   else if (desc->exec == FOT_EXEC_HIER)
-    kname = (plan->variant & kVariantSplit) ? "split write-back"
+    kname = (plan->variant & kVariantSplit)
+                ? ((plan->variant & kVariantPipe) ? "split write-back" : "split write-back, direct")
             : (plan->variant & kVariantPipe) ? "pipelined, block flags"
             : (plan->variant & kVariantStage) ? "simple persistent"
                                                : "simple persistent, direct reads";
@@ -549,9 +554,13 @@ static int run_plan(fot_problem *p, fot_plan *plan, uint32_t iterations, cudaStr
     if ((uint64_t)iterations * plan->n_blocks + (uint64_t)plan->per_sm * sms >= 0xFFFFFFFFull)
       return fail(FOT_ERR_LIMIT, "too many tiles in one launch");
     const HierPlanDev P = plan->dev(iterations);
-    // the split kernel runs one iteration per launch over the plan's blocks
-    const uint32_t tiles = (plan->variant & kVariantSplit) ? plan->n_blocks : P.total_tiles;
-    const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)(plan->per_sm * sms));
+    // the split kernels run one iteration per launch over the plan's blocks:
+    // persistent CTAs (staged form) or one CTA per block (direct form)
+    const bool split = plan->variant & kVariantSplit;
+    const uint32_t tiles = split ? plan->n_blocks : P.total_tiles;
+    const uint32_t grid = (split && !(plan->variant & kVariantPipe))
+                              ? plan->n_blocks
+                              : std::min<uint32_t>(tiles, (uint32_t)(plan->per_sm * sms));
     return ops->run_hier(d, P, soa, plan->threads, plan->variant, grid, plan->smem, st);
   }
   const HierPlanDev P = plan->dev(1);
@@ -582,12 +591,10 @@ int fot_sync(fot_problem *p, void *stream) {
     Ctl c{};
     FOT_CUDA(cudaMemcpy(&c, plan->ctl.ptr, sizeof(Ctl), cudaMemcpyDeviceToHost));
     if (!c.error) continue;
-    // the run stopped early: restart the plan's queue, flags and arrival
-    // counters from zero
+    // the run stopped early: restart the plan's queue and flags from zero
     ++failed;
     FOT_CUDA(cudaMemset(plan->ctl.ptr, 0, sizeof(Ctl)));
     if (plan->block_done.ptr) FOT_CUDA(cudaMemset(plan->block_done.ptr, 0, (size_t)plan->n_blocks * 4));
-    if (plan->counter.ptr) FOT_CUDA(cudaMemset(plan->counter.ptr, 0, (size_t)plan->n_slots * 4));
   }
   if (failed)
     return fail(FOT_ERR_DEVICE, "%d hierarchical plan(s) stopped early: a wait of the persistent "

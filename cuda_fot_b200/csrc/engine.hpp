@@ -30,9 +30,10 @@ struct SmemLayout {
 // pipelined persistent kernel (warp-specialised: tile records by bulk copy,
 // double-buffered staging, per-point gather of the increments), launched
 // with 64 threads more than `threads` for its two control warps; bit 2 = that
-// kernel with three tile-record slots (else two); bit 3 = the split
-// write-back kernel (hier_split.cuh; with bit 1, same control warps and slot
-// counts, one launch per iteration).
+// kernel with three tile-record slots (else two); bit 3 = split write-back
+// (hier_split.cuh, one launch per iteration): with bit 1 the warp-specialised
+// staged form (same control warps and slot counts), without it the direct
+// form (one CTA per tile, rows gathered straight from HBM/L2).
 constexpr uint32_t kVariantStage = 1u, kVariantPipe = 2u, kVariantSlots3 = 4u, kVariantSplit = 8u;
 
 struct LoopOps {
@@ -119,8 +120,9 @@ struct fot_plan {
   fot::DevBuf build_perm; // position -> cell index before the build
   fot::DevBuf rec, rec_off; // tile records (see plan.cu)
   fot::DevBuf block_done;   // per block: completed iterations (pipelined executor)
-  // split write-back kernel: partial-sum slots, arrival counters, tile order
-  fot::DevBuf partial, counter, launch;
+  // split write-back kernels: two partial-sum buffers, the shared points and
+  // their slot ranges, the tiles' launch order
+  fot::DevBuf partial, comb_point, comb_base, launch;
   uint32_t n_slots = 0, n_shared_points = 0;
   uint32_t rec_cap = 0;
   uint32_t cap[2] = {0, 0};

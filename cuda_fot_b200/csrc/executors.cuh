@@ -74,10 +74,15 @@ struct HierPlanDev {
   uint32_t outbuf_off;         // first prefetched-output-row slot
   uint32_t outbuf_bytes;       // bytes of one output-row slot
   unsigned int *block_done;    // per block: completed iterations (relative to ctl->base)
-  // split write-back kernel
+  // split write-back kernels
   const uint32_t *launch;      // tile -> block (formation order)
-  void *partial;               // partial-sum slots (AOS rows of point dataset 0's type)
-  unsigned int *counter;       // arrivals per shared point (at its first slot)
+  void *partial;               // 2 x n_slots partial-sum rows (AOS, point dataset 0's type)
+  const uint32_t *comb_point;  // shared point g -> point number
+  const uint32_t *comb_base;   // shared point g -> its slots [base[g], base[g+1])
+  uint32_t n_slots, n_shared;
+  // per launch: tiles run (0: combine only), the buffer they fill, whether
+  // the other buffer (previous iteration) is combined, CTAs doing that
+  uint32_t tiles_on, put_buf, comb_on, comb_ctas;
 };
 
 // Direct (cell) data of one cell: SOA with stride n_cells.

@@ -1,41 +1,45 @@
-// The split write-back hierarchical-colour kernel (variant kVariantSplit).
+// The split write-back hierarchical-colour kernels (variant kVariantSplit).
 //
 // The coloured replay of a plan (blocks in block-colour order; in a block,
 // cells in thread-colour order accumulate into a zeroed per-block sum; then
 // out[p] += sum for each written point) fixes, for every point p, the order
 // out[p] = ((out[p] + S_b1) + S_b2) + ... over the blocks b1 < b2 < ... (plan
-// order) that write p.  This kernel reproduces that order without making any
-// tile wait for another:
+// order) that write p.  These kernels reproduce that order without making
+// any tile wait for another:
 //   * a point written by ONE block (private) gets out[p] += S_b as soon as
 //     the block's sum is ready -- a fire-and-forget L2 reduction (RED.F64) for
 //     FP64 data, whose single rounding equals the replay's add; FP32 data
 //     (atomics there flush subnormals) take a load-add-store;
-//   * a point written by several blocks (shared) gets each block's S_b stored
-//     into the block's partial-sum slot; the block that arrives LAST at the
-//     point's counter (acquire-release atomic) adds out[p] + S_b1 + S_b2 ...
-//     in plan order and resets the counter.
+//   * a point written by several blocks (shared) gets S_b stored into the
+//     point's slot for that block (plain stores, one buffer per iteration
+//     parity); the NEXT launch -- the next iteration's, or the flush launch
+//     that ends a run -- adds out[p] + S_b1 + S_b2 ... in plan order while its
+//     own tiles fill the other buffer.  Private and shared points are
+//     disjoint, so the combine never races with the tiles.
 // Block colours therefore fix the summation order but never stall a tile.
-// One launch runs ONE iteration (the partial slots and counters are reused
-// by the next one); consecutive iterations are chained with programmatic
-// dependent launch: every CTA allows the next grid to launch at once, and the
-// next grid's tiles stage and compute (they only read datasets the loop never
-// writes) before they wait (griddepcontrol.wait) for this grid to complete
-// and only then write.  Loops that write cell data wait before computing.
+// One launch runs ONE iteration; consecutive launches are chained with
+// programmatic dependent launch: every CTA lets the next grid launch at once,
+// and the next grid's tiles gather and compute (they only read datasets the
+// loop never writes) before they wait (griddepcontrol.wait) for this grid to
+// complete and only then write.  Loops that write cell data wait before
+// computing.
 //
-// A CTA runs T compute threads and two control warps over its tiles (tile i
-// of CTA c is launch[c + i * gridDim.x]: at any moment the GPU works on a
-// window of consecutive tiles in formation order, so blocks sharing points
-// run close together and their partial sums meet in L2):
-//   * the RECORD warp bulk-copies each tile's record (plan.cu, step 4b) into
-//     one of kRecSlots record slots (TMA engine, no multicast) and refills a
-//     slot once the compute threads are done with its tile;
-//   * the STAGING warp gathers a tile's read rows into one of two row slots
-//     with cp.async as soon as the compute phase that used the slot ends;
-//   * the COMPUTE threads compute each cell's per-slot increments into
-//     shared memory, then, per written point, sum its contributions in
-//     thread-colour order (bit-identical to the replay) and write it back.
-// Every wait between the roles is bounded (about two seconds); on a timeout
-// the kernel sets kErrWaitLimit in Ctl::error and returns.
+// Two forms:
+//   * k_hier_dsplit (direct): one CTA per tile, one thread per cell; each
+//     thread gathers its cell's rows straight from HBM/L2 through the
+//     plan-ordered mapping (like the atomic executor: thousands of
+//     independent gathers in flight per SM), computes into shared memory, and
+//     the block's sums go out as above.  Extra CTAs at the front of the grid
+//     do the combine.
+//   * k_hier_split (staged): persistent CTAs of T compute threads and two
+//     control warps; the RECORD warp bulk-copies each tile's record (plan.cu,
+//     step 4b) into one of kRecSlots slots (TMA engine, no multicast), the
+//     STAGING warp gathers the tile's read rows into one of two row slots
+//     with cp.async, the compute threads compute from shared memory.  Tile i
+//     of CTA c is launch[c + i * gridDim.x]; every CTA's compute threads
+//     combine one chunk of the shared points after their wait.  Every wait
+//     between the roles is bounded (about two seconds); on a timeout the
+//     kernel sets kErrWaitLimit in Ctl::error and returns.
 #pragma once
 
 #include <cstdint>
@@ -56,28 +60,121 @@ __device__ __forceinline__ void griddep_wait() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
-__device__ __forceinline__ unsigned int atom_add_acq_rel_gpu(unsigned int *p, unsigned int v) {
-  unsigned int old;
-  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
-  return old;
+// Shared points [g0, g1) of the previous launch's buffer: out[p] plus the
+// blocks' sums in plan order (thread t of nt).
+template <class L, bool SOA>
+__device__ __forceinline__ void combine_shared(const LoopData &d, const HierPlanDev &P, uint32_t g0,
+                                               uint32_t g1, uint32_t t, uint32_t nt) {
+  using out_t = typename L::out_t;
+  constexpr int K = L::kOut;
+  const out_t *part = static_cast<const out_t *>(P.partial) + (size_t)(P.put_buf ^ 1u) * P.n_slots * K;
+  out_t *out = static_cast<out_t *>(d.out);
+  for (uint32_t g = g0 + t; g < g1; g += nt) {
+    const uint32_t p = P.comb_point[g], e0 = P.comb_base[g], e1 = P.comb_base[g + 1];
+    out_t o[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) o[k] = __ldcg(out + out_index(SOA, d.n_points[0], p, K, k));
+    for (uint32_t e = e0; e < e1; ++e)
+#pragma unroll
+      for (int k = 0; k < K; ++k) o[k] += __ldcg(part + (size_t)e * K + k);
+#pragma unroll
+    for (int k = 0; k < K; ++k) __stcg(out + out_index(SOA, d.n_points[0], p, K, k), o[k]);
+  }
 }
 
-// The split part of a tile record (plan.cu, build_split), at the record's
-// dependency offset (split plans have no dependency list).
-struct SplitView {
-  uint32_t n_sh, sh_off;
-  const uint16_t *sh_of;   // per written point: index among the shared points, 0xFFFF private
-  const uint16_t *sl_off;  // n_sh + 1
-  const uint32_t *sl;      // slots of each shared point's blocks, plan order
-  __device__ __forceinline__ SplitView(const uint32_t *at, uint32_t n0) {
-    n_sh = at[0];
-    sh_off = at[1];
-    sh_of = reinterpret_cast<const uint16_t *>(at + 2);
-    sl_off = sh_of + n0;
-    const uintptr_t e = reinterpret_cast<uintptr_t>(sl_off + n_sh + 1);
-    sl = reinterpret_cast<const uint32_t *>((e + 3) & ~uintptr_t(3));
+__device__ __forceinline__ void comb_chunk(uint32_t n, uint32_t c, uint32_t parts, uint32_t &g0,
+                                           uint32_t &g1) {
+  g0 = (uint32_t)((uint64_t)n * c / parts);
+  g1 = (uint32_t)((uint64_t)n * (c + 1) / parts);
+}
+
+// Written point j of a tile (threads j = t, t + T, ...): sum its contributions
+// in thread-colour order from the increments in shared memory, then add it
+// (private) or store it into its slot of this launch's buffer (shared).
+template <class L, bool SOA, int T>
+__device__ __forceinline__ void split_writeback(const LoopData &d, const HierPlanDev &P,
+                                                const RecView<L> &m, const typename L::out_t *inc,
+                                                uint32_t t) {
+  using out_t = typename L::out_t;
+  constexpr int D = L::kDim, K = L::kOut;
+  out_t *out = static_cast<out_t *>(d.out);
+  out_t *put = static_cast<out_t *>(P.partial) + (size_t)P.put_buf * P.n_slots * K;
+  const uint32_t *wslot = m.dep;  // split plans: the record's slot list
+  for (uint32_t j = t; j < m.n0; j += T) {
+    out_t acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = out_t(0);
+    const uint32_t e0 = m.pc_off[j], e1 = m.pc_off[j + 1];
+    for (uint32_t e = e0; e < e1; ++e) {
+      const uint32_t ie = m.pc_idx[e];
+#pragma unroll
+      for (int k = 0; k < K; ++k) acc[k] += inc[k * D * T + ie];
+    }
+    const uint32_t p = m.pts0[j];
+    const uint32_t ws = wslot[j];
+    if (ws == 0xFFFFFFFFu) {
+      // private point: this block alone writes it in this iteration
+      if constexpr (sizeof(out_t) == 8) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) atomicAdd(out + out_index(SOA, d.n_points[0], p, K, k), acc[k]);
+      } else {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          out_t *o = out + out_index(SOA, d.n_points[0], p, K, k);
+          __stcg(o, __ldcg(o) + acc[k]);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < K; ++k) __stcg(put + (size_t)ws * K + k, acc[k]);
+    }
   }
-};
+}
+
+// Direct form: CTAs [0, comb_ctas) combine the previous buffer, the others
+// run one tile each.
+template <class L, bool SOA, int T>
+__global__ void __launch_bounds__(T, hier_min_blocks<L, T>()) k_hier_dsplit(LoopData d, HierPlanDev P) {
+  using out_t = typename L::out_t;
+  using read_t = typename L::read_t;
+  constexpr int D = L::kDim, K = L::kOut;
+  extern __shared__ __align__(16) unsigned char smem[];
+  out_t *const inc = reinterpret_cast<out_t *>(smem);
+  const uint32_t tid = threadIdx.x;
+  griddep_launch_dependents();
+  if (blockIdx.x < P.comb_ctas) {
+    griddep_wait();
+    if (P.comb_on) {
+      uint32_t g0, g1;
+      comb_chunk(P.n_shared, blockIdx.x, P.comb_ctas, g0, g1);
+      combine_shared<L, SOA>(d, P, g0, g1, tid, T);
+    }
+    return;
+  }
+  const RecView<L> m(P.rec + P.rec_off[P.launch[blockIdx.x - P.comb_ctas]]);
+  if constexpr (L::kWritesCell) griddep_wait();  // the previous iteration may still write cell data
+  if (tid < m.ncell) {
+    const uint32_t pos = m.start + tid;
+    GlobalRows<L, SOA> rows;
+    load_row<D>(d.map[0], pos, rows.p[0]);
+    if constexpr (L::kHasClass1) load_row<D>(d.map[1], pos, rows.p[1]);
+    static_for_read<L>([&](auto r) {
+      constexpr int R = decltype(r)::value;
+      rows.base[R] = static_cast<const read_t *>(d.point[L::read_set(R)]);
+      rows.np[R] = d.n_points[L::read_set(R)];
+    });
+    out_t v[D][K];
+    Direct dir{d.cell, pos, d.n_cells};
+    L::cell(rows, dir, v);
+#pragma unroll
+    for (int q = 0; q < D; ++q)
+#pragma unroll
+      for (int k = 0; k < K; ++k) inc[(k * D + q) * T + tid] = v[q][k];
+  }
+  __syncthreads();
+  if constexpr (!L::kWritesCell) griddep_wait();  // the previous iteration's writes are visible
+  split_writeback<L, SOA, T>(d, P, m, inc, tid);
+}
 
 template <class L, bool SOA, int T, uint32_t kRecSlots>
 __global__ void __launch_bounds__(T + 64) __maxnreg__(L::kRegCap)
@@ -98,8 +195,6 @@ __global__ void __launch_bounds__(T + 64) __maxnreg__(L::kRegCap)
   unsigned char *const rec_base = smem;
   unsigned char *const rows_base = smem + P.rows_off;
   out_t *const inc = reinterpret_cast<out_t *>(smem + P.inc_off);
-  out_t *__restrict__ out = static_cast<out_t *>(d.out);
-  out_t *__restrict__ partial = static_cast<out_t *>(P.partial);
 
   griddep_launch_dependents();
   if (tid == 0) {
@@ -182,7 +277,8 @@ __global__ void __launch_bounds__(T + 64) __maxnreg__(L::kRegCap)
     cp_async_wait_all();
   } else {
     // --------------------------------------------------------------- compute
-    bool waited = false;  // griddepcontrol.wait done
+    bool waited = false;    // griddepcontrol.wait done
+    bool combined = false;  // this CTA's combine chunk done
     for (uint32_t i = 0;; ++i) {
       const uint32_t s = i % kRecSlots, b = i & 1u, ph = (i >> 1) & 1u;
       const bool ok_rows = mbar_wait_or_stop(&s_rows_full[b], ph, &s_stop);
@@ -231,56 +327,16 @@ __global__ void __launch_bounds__(T + 64) __maxnreg__(L::kRegCap)
         griddep_wait();
         waited = true;
       }
-      const SplitView sv(m.dep, m.n0);
-      for (uint32_t j = tid; j < m.n0; j += T) {
-        out_t acc[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) acc[k] = out_t(0);
-        const uint32_t e0 = m.pc_off[j], e1 = m.pc_off[j + 1];
-        for (uint32_t e = e0; e < e1; ++e) {
-          const uint32_t ie = m.pc_idx[e];
-#pragma unroll
-          for (int k = 0; k < K; ++k) acc[k] += inc[k * D * T + ie];
-        }
-        const uint32_t p = m.pts0[j];
-        const uint32_t sh = sv.sh_of[j];
-        if (sh == 0xFFFFu) {
-          // private point: this block alone writes it in this iteration
-          if constexpr (sizeof(out_t) == 8) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) atomicAdd(out + out_index(SOA, d.n_points[0], p, K, k), acc[k]);
-          } else {
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-              out_t *o = out + out_index(SOA, d.n_points[0], p, K, k);
-              __stcg(o, __ldcg(o) + acc[k]);
-            }
-          }
-        } else {
-          // shared point: publish the block's sum; the last block to arrive
-          // adds all sums to out[p] in plan order
-          const uint32_t slot = sv.sh_off + sh;
-#pragma unroll
-          for (int k = 0; k < K; ++k) __stcg(partial + (size_t)slot * K + k, acc[k]);
-          const uint32_t l0 = sv.sl_off[sh], l1 = sv.sl_off[sh + 1];
-          unsigned int *cnt = P.counter + sv.sl[l0];
-          const unsigned int prev = atom_add_acq_rel_gpu(cnt, 1u);
-          if (prev + 1 == l1 - l0) {
-            out_t o[K];
-#pragma unroll
-            for (int k = 0; k < K; ++k) o[k] = __ldcg(out + out_index(SOA, d.n_points[0], p, K, k));
-            for (uint32_t e = l0; e < l1; ++e) {
-              const out_t *q = partial + (size_t)sv.sl[e] * K;
-#pragma unroll
-              for (int k = 0; k < K; ++k) o[k] += __ldcg(q + k);
-            }
-#pragma unroll
-            for (int k = 0; k < K; ++k) __stcg(out + out_index(SOA, d.n_points[0], p, K, k), o[k]);
-            // every block of this point has arrived: ready for the next launch
-            *cnt = 0u;
-          }
+      if (!combined) {
+        // this CTA's share of the previous buffer's shared points
+        combined = true;
+        if (P.comb_on) {
+          uint32_t g0, g1;
+          comb_chunk(P.n_shared, blockIdx.x, gridDim.x, g0, g1);
+          combine_shared<L, SOA>(d, P, g0, g1, tid, T);
         }
       }
+      split_writeback<L, SOA, T>(d, P, m, inc, tid);
       __syncwarp();
       if (lane == 0) mbar_arrive(&s_tile_done[s]);
       // the increments buffer is reused by the next tile

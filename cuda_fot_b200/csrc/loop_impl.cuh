@@ -52,10 +52,22 @@ template <bool SOA, uint32_t SLOTS> const void *split_kernel(uint32_t threads) {
   return nullptr;
 }
 
+template <bool SOA> const void *dsplit_kernel(uint32_t threads) {
+  switch (threads) {
+  case 128: return reinterpret_cast<const void *>(&k_hier_dsplit<L, SOA, 128>);
+  case 256: return reinterpret_cast<const void *>(&k_hier_dsplit<L, SOA, 256>);
+  case 512: return reinterpret_cast<const void *>(&k_hier_dsplit<L, SOA, 512>);
+  }
+  return nullptr;
+}
+
 // variant: kVariantStage (staged reads), kVariantPipe (pipelined kernel),
-// kVariantSplit (split write-back kernel)
+// kVariantSplit (split write-back kernels: staged with kVariantPipe, else
+// direct)
 const void *kernel_for(int exec, bool soa, uint32_t threads, uint32_t variant) {
   if (exec == FOT_EXEC_ATOMIC) return nullptr;
+  if (exec == FOT_EXEC_HIER && (variant & kVariantSplit) && !(variant & kVariantPipe))
+    return soa ? dsplit_kernel<true>(threads) : dsplit_kernel<false>(threads);
   if (exec == FOT_EXEC_HIER && (variant & kVariantSplit)) {
     if (variant & kVariantSlots3) return soa ? split_kernel<true, 3>(threads) : split_kernel<false, 3>(threads);
     return soa ? split_kernel<true, 2>(threads) : split_kernel<false, 2>(threads);
@@ -85,24 +97,38 @@ int run_hier(const LoopData &d, const HierPlanDev &P, bool soa, uint32_t threads
   void *args[] = {const_cast<LoopData *>(&d), const_cast<HierPlanDev *>(&P)};
   const uint32_t block = (variant & kVariantPipe) ? threads + 64 : threads;
   if (variant & kVariantSplit) {
-    // one launch per iteration; from the second on, programmatic dependent
-    // launch lets the next iteration's tiles stage and compute while this
-    // one drains (the kernel waits before it writes).  The first launch of
-    // a call is fully stream-ordered: whatever precedes it may write the
-    // datasets it reads.
+    // One launch per iteration.  Launch `it` fills partial buffer it & 1 and
+    // combines buffer (it - 1) & 1 (direct form: in comb_ctas extra CTAs;
+    // staged form: in every CTA after its wait); a last, combine-only launch
+    // of the direct kernel flushes the final iteration's buffer.  From the
+    // second launch on, programmatic dependent launch lets the next grid
+    // gather and compute while this one drains (the kernels wait before
+    // they write); the first launch of a call is fully stream-ordered:
+    // whatever precedes it may write the datasets it reads.
     const uint32_t iters = P.n_blocks ? P.total_tiles / P.n_blocks : 0;
+    const bool direct = !(variant & kVariantPipe);
+    const uint32_t comb_ctas = P.n_shared ? (P.n_shared + 4 * threads - 1) / (4 * threads) : 0;
+    const void *flush = soa ? dsplit_kernel<true>(threads) : dsplit_kernel<false>(threads);
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(block);
-    cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
-    for (uint32_t it = 0; it < iters; ++it) {
+    HierPlanDev Q = P;
+    void *qargs[] = {const_cast<LoopData *>(&d), &Q};
+    for (uint32_t it = 0; it <= iters; ++it) {
+      const bool last = it == iters;
+      if (last && P.n_shared == 0) break;
+      Q.tiles_on = last ? 0u : 1u;
+      Q.put_buf = it & 1u;
+      Q.comb_on = it > 0 && P.n_shared > 0;
+      Q.comb_ctas = (direct || last) && Q.comb_on ? comb_ctas : 0u;
+      cfg.gridDim = dim3(last ? Q.comb_ctas : grid + (direct ? Q.comb_ctas : 0u));
+      cfg.blockDim = dim3(last ? threads : block);
+      cfg.dynamicSmemBytes = last ? 0 : smem;
       cfg.attrs = it > 0 ? attr : nullptr;
       cfg.numAttrs = it > 0 ? 1 : 0;
-      FOT_CUDA(cudaLaunchKernelExC(&cfg, k, args));
+      FOT_CUDA(cudaLaunchKernelExC(&cfg, last ? flush : k, qargs));
     }
     return FOT_OK;
   }
@@ -142,6 +168,13 @@ void smem_layout(uint32_t cap0, uint32_t cap1, uint32_t variant, uint32_t rec_ca
   auto a16 = [](size_t v) { return (v + 15) & ~size_t(15); };
   SmemLayout s;
   size_t off = 0;
+  if ((variant & kVariantSplit) && !(variant & kVariantPipe)) {
+    // direct split write-back: the per-slot increments only
+    s.inc_off = 0;
+    s.total = a16((size_t)L::kOut * L::kDim * threads * sizeof(out_t));
+    *out = s;
+    return;
+  }
   if (variant & kVariantPipe) {
     // 2 or 3 tile-record slots, 2 read-row slots, the per-slot increments, 2
     // prefetched-output-row slots (AOS output rows of a multiple of 16 bytes;

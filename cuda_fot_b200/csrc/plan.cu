@@ -294,19 +294,16 @@ __global__ void k_gather_plan(GatherArgs g) {
 // accumulation (res_calc.hpp:328-339).
 // dep lists the blocks sharing a written point with this one (the conflict
 // graph); bit 31 marks those of an earlier block colour.
-// Plans of the split write-back kernel (hier_split.cuh) have no dep list;
-// in its place, at the same offset, comes the block's split record
-// (build_split below):
-//   u32 n_sh, u32 sh_off, u16 sh_of[n0], u16 sl_off[n_sh + 1], (pad to 4),
-//   u32 sl[sl_off[n_sh]], zero padding to 16 bytes
+// Plans of the split write-back kernels (hier_split.cuh) have no dep list;
+// in its place, at the same offset, comes u32 wslot[n0] (build_split below),
+// then zero padding to 16 bytes.
 // ---------------------------------------------------------------------------
 struct RecordArgs {
   const uint32_t *block_start, *block_wait, *pts_off[2], *pts[2], *rec_off;
   const uint16_t *lidx[2];
   const uint8_t *ntcol;
   const uint32_t *dep_off, *dep;
-  const unsigned char *split;      // split records, or null
-  const uint32_t *split_off;       // n_blocks+1 byte offsets into split
+  const uint32_t *wslot;           // split plans: per written point (pts_off order), or null
   unsigned char *rec;
   uint32_t n_cells, threads;
   int n_class, D;
@@ -381,10 +378,11 @@ __global__ void k_build_records(RecordArgs a) {
   uint32_t *dep = reinterpret_cast<uint32_t *>(r + dep_at);
   for (uint32_t i = threadIdx.x; i < ndep; i += blockDim.x) dep[i] = a.dep[a.dep_off[b] + i];
   uint32_t used = dep_at + 4 * ndep;
-  if (a.split) {
-    const uint32_t s0 = a.split_off[b], sn = a.split_off[b + 1] - s0;
-    for (uint32_t i = threadIdx.x; i < sn; i += blockDim.x) r[used + i] = a.split[s0 + i];
-    used += sn;
+  if (a.wslot) {
+    uint32_t *w = reinterpret_cast<uint32_t *>(r + used);
+    const uint32_t *src = a.wslot + a.pts_off[0][b];
+    for (uint32_t i = threadIdx.x; i < n[0]; i += blockDim.x) w[i] = src[i];
+    used += 4 * n[0];
   }
   for (uint32_t i = used + threadIdx.x; i < a.rec_off[b + 1] - a.rec_off[b]; i += blockDim.x) r[i] = 0;
 }
@@ -513,20 +511,16 @@ static int colour_blocks(const DevBuf &pad0, const DevBuf &cnt0, uint32_t nfb, u
 }
 
 // Split write-back data of a plan (hier_split.cuh).  A written point of a
-// block is PRIVATE when no other block writes it, else SHARED.  Every
-// (shared point, block) pair gets a partial-sum slot; the slots of one block
-// are consecutive (from sh_off) in the block's point order.  The blocks
-// writing a shared point, in plan order -- block-colour order, the order in
-// which the coloured replay adds their sums -- give its slot list.  Output
-// per block (the split record of the tile record layout above):
-//   u32 n_sh, u32 sh_off, u16 sh_of[n0] (index among the block's shared
-//   points, 0xFFFF: private), u16 sl_off[n_sh + 1], pad to 4,
-//   u32 sl[] (for each shared point, the slots of its blocks in plan order).
+// block is PRIVATE when no other block writes it, else SHARED.  Shared points
+// are numbered g = 0, 1, ... in point order; shared point g owns the
+// partial-sum slots [base[g], base[g + 1]), one per block writing it, in
+// plan order -- block-colour order, the order in which the coloured replay
+// adds the blocks' sums.  Per block, wslot[j] is the slot of its j-th written
+// point (0xFFFFFFFF: private); per shared point, its point number and base.
 struct SplitRecords {
-  std::vector<unsigned char> bytes;
-  std::vector<uint32_t> off;  // n_blocks + 1
+  std::vector<uint32_t> wslot;            // per (block, written point), plan order
+  std::vector<uint32_t> point, base;      // n_shared, n_shared + 1
   uint32_t n_slots = 0;
-  uint32_t n_shared_points = 0;
 };
 
 static int build_split(const std::vector<uint32_t> &pts0, const std::vector<uint32_t> &off0,
@@ -538,62 +532,23 @@ static int build_split(const std::vector<uint32_t> &pts0, const std::vector<uint
     if (pts0[j] >= n_points) return fail(FOT_ERR_STATE, "plan point %u out of range", pts0[j]);
     ++deg[pts0[j]];
   }
-  // slot of every (block, shared point) pair; slots of a block consecutive
-  std::vector<uint32_t> slot(n_pairs, 0xFFFFFFFFu), sh_off(nfb + 1, 0);
-  uint32_t next = 0;
-  for (uint32_t b = 0; b < nfb; ++b) {
-    sh_off[b] = next;
-    for (uint32_t j = off0[b]; j < off0[b + 1]; ++j)
-      if (deg[pts0[j]] > 1) slot[j] = next++;
-  }
-  sh_off[nfb] = next;
-  // slot lists per shared point, filled in block (plan) order
-  std::vector<uint32_t> lstart(n_points + 1, 0);
-  uint32_t n_shared = 0;
-  for (uint32_t q = 0; q < n_points; ++q) {
-    lstart[q + 1] = lstart[q] + (deg[q] > 1 ? deg[q] : 0);
-    n_shared += deg[q] > 1;
-  }
-  std::vector<uint32_t> list(lstart[n_points]), fill(lstart.begin(), lstart.end() - 1);
-  for (uint32_t b = 0; b < nfb; ++b)
-    for (uint32_t j = off0[b]; j < off0[b + 1]; ++j)
-      if (slot[j] != 0xFFFFFFFFu) list[fill[pts0[j]]++] = slot[j];
-  out.bytes.clear();
-  out.off.assign(nfb + 1, 0);
-  std::vector<uint16_t> sh_of, sl_off;
-  std::vector<uint32_t> sl;
-  for (uint32_t b = 0; b < nfb; ++b) {
-    const uint32_t n0 = off0[b + 1] - off0[b];
-    const uint32_t n_sh = sh_off[b + 1] - sh_off[b];
-    sh_of.assign(n0, 0xFFFFu);
-    sl_off.assign(n_sh + 1, 0);
-    sl.clear();
-    uint32_t k = 0;
-    for (uint32_t i = 0; i < n0; ++i) {
-      const uint32_t j = off0[b] + i;
-      if (slot[j] == 0xFFFFFFFFu) continue;
-      const uint32_t q = pts0[j];
-      sh_of[i] = (uint16_t)k;
-      for (uint32_t e = lstart[q]; e < lstart[q + 1]; ++e) sl.push_back(list[e]);
-      if (sl.size() > 0xFFFFu) return fail(FOT_ERR_LIMIT, "block %u: too many shared contributions", b);
-      sl_off[++k] = (uint16_t)sl.size();
+  std::vector<uint32_t> g_of(n_points, 0xFFFFFFFFu);
+  out.point.clear();
+  out.base.assign(1, 0);
+  for (uint32_t q = 0; q < n_points; ++q)
+    if (deg[q] > 1) {
+      g_of[q] = (uint32_t)out.point.size();
+      out.point.push_back(q);
+      out.base.push_back(out.base.back() + deg[q]);
     }
-    const size_t at = out.bytes.size();
-    size_t nb = 8 + 2 * (size_t)n0 + 2 * (size_t)(n_sh + 1);
-    nb = (nb + 3) & ~size_t(3);
-    const size_t sl_at = nb;
-    nb += 4 * sl.size();
-    out.bytes.resize(at + nb, 0);
-    unsigned char *w = out.bytes.data() + at;
-    const uint32_t hdr[2] = {n_sh, sh_off[b]};
-    std::memcpy(w, hdr, 8);
-    std::memcpy(w + 8, sh_of.data(), 2 * (size_t)n0);
-    std::memcpy(w + 8 + 2 * (size_t)n0, sl_off.data(), 2 * (size_t)(n_sh + 1));
-    if (!sl.empty()) std::memcpy(w + sl_at, sl.data(), 4 * sl.size());
-    out.off[b + 1] = (uint32_t)out.bytes.size();
-  }
-  out.n_slots = next;
-  out.n_shared_points = n_shared;
+  std::vector<uint32_t> fill(out.base.begin(), out.base.end() - 1);
+  out.wslot.assign(n_pairs, 0xFFFFFFFFu);
+  for (uint32_t b = 0; b < nfb; ++b)  // plan order: each point's slots in colour order
+    for (uint32_t j = off0[b]; j < off0[b + 1]; ++j) {
+      const uint32_t g = g_of[pts0[j]];
+      if (g != 0xFFFFFFFFu) out.wslot[j] = fill[g]++;
+    }
+  out.n_slots = out.base.back();
   return FOT_OK;
 }
 
@@ -763,7 +718,7 @@ int build_hier_plan(fot_problem *p, fot_plan *plan) {
       }
       dep_off[b + 1] = (uint32_t)dep.size();
     }
-    DevBuf d_dep_off, d_dep, d_split, d_split_off;
+    DevBuf d_dep_off, d_dep, d_split;
     FOT_TRY(upload(d_dep_off, dep_off));
     FOT_TRY(upload(d_dep, dep));
     SplitRecords sr;
@@ -771,19 +726,18 @@ int build_hier_plan(fot_problem *p, fot_plan *plan) {
       std::vector<uint32_t> h_pts0;
       FOT_TRY(download(h_pts0, plan->pts[0], h_off[0][nfb]));
       FOT_TRY(build_split(h_pts0, h_off[0], p->n_points[0], sr));
-      FOT_TRY(upload(d_split, sr.bytes));
-      FOT_TRY(upload(d_split_off, sr.off));
-      // partial sums (AOS rows of the incremented dataset's element type),
-      // one arrival counter per shared point (at its first slot), and the
-      // launch order of the tiles: formation order, so that blocks sharing
-      // points run close together in time
+      FOT_TRY(upload(d_split, sr.wslot));
+      // two buffers of partial sums (AOS rows of the incremented dataset's
+      // element type; a launch fills one while it combines the other), the
+      // shared points with their slot ranges, and the launch order of the
+      // tiles: formation order, so that neighbouring blocks run together
       const size_t row = (size_t)p->info.point_dim[0] * p->info.point_type_size[0];
-      FOT_TRY(plan->partial.alloc((size_t)sr.n_slots * row));
-      FOT_TRY(plan->counter.alloc((size_t)sr.n_slots * 4));
-      FOT_CUDA(cudaMemset(plan->counter.ptr, 0, (size_t)sr.n_slots * 4));
+      FOT_TRY(plan->partial.alloc(2 * (size_t)sr.n_slots * row));
+      FOT_TRY(upload(plan->comb_point, sr.point));
+      FOT_TRY(upload(plan->comb_base, sr.base));
       FOT_TRY(upload(plan->launch, final_of));
       plan->n_slots = sr.n_slots;
-      plan->n_shared_points = sr.n_shared_points;
+      plan->n_shared_points = (uint32_t)sr.point.size();
     }
     std::vector<uint32_t> rec_off(nfb + 1, 0);
     uint32_t rec_cap = 0;
@@ -792,8 +746,7 @@ int build_hier_plan(fot_problem *p, fot_plan *plan) {
       const uint32_t n0 = h_off[0][b + 1] - h_off[0][b];
       const uint32_t n1 = n_class > 1 ? h_off[1][b + 1] - h_off[1][b] : 0;
       uint32_t padded = record_bytes(ncell, n0, n1, D, n_class, dep_off[b + 1] - dep_off[b]);
-      if (split)
-        padded = (record_dep_offset(ncell, n0, n1, D, n_class) + (sr.off[b + 1] - sr.off[b]) + 15) & ~15u;
+      if (split) padded = (record_dep_offset(ncell, n0, n1, D, n_class) + 4 * n0 + 15) & ~15u;
       rec_cap = std::max(rec_cap, padded);
       rec_off[b + 1] = rec_off[b] + padded;
     }
@@ -810,8 +763,7 @@ int build_hier_plan(fot_problem *p, fot_plan *plan) {
     ra.threads = hier_threads(B);
     ra.dep_off = d_dep_off.as<uint32_t>();
     ra.dep = d_dep.as<uint32_t>();
-    ra.split = split ? d_split.as<unsigned char>() : nullptr;
-    ra.split_off = split ? d_split_off.as<uint32_t>() : nullptr;
+    ra.wslot = split ? d_split.as<uint32_t>() : nullptr;
     ra.ntcol = plan->block_ntcol.as<uint8_t>();
     ra.rec = plan->rec.as<unsigned char>();
     ra.n_cells = n;

@@ -75,7 +75,8 @@ extern "C" {
 #define FOT_PLAN_NO_AGGREGATE 1u /* atomic executor: no warp aggregation */
 #define FOT_PLAN_USE_PARTITION 2u /* hierarchical: blocks from the partition */
 #define FOT_PLAN_DIRECT_READS 4u  /* hierarchical: gather read rows from HBM/L2 instead of
-                                     staging them in shared memory */
+                                     staging them in shared memory (persistent executor:
+                                     the direct split write-back kernel, one CTA per block) */
 #define FOT_PLAN_SIMPLE_TILES 8u  /* persistent hierarchical: one tile at a time with a
                                      barrier per thread colour (no pipelining) */
 #define FOT_PLAN_BLOCK_FLAGS 16u  /* persistent hierarchical: the pipelined kernel whose tiles

@@ -124,8 +124,8 @@ def test_single_kind_atomic_batch_matches_serial(loop):
     for md, p in zip(mds, probs):
         ser, ser_cd = O.serial(md, 3)
         assert rel_err(p.point_weights(0), ser[0]) <= tol(md.loop)
-        for j, ref in enumerate(ser_cd):  # lulesh's written element volumes
-            assert bitwise_equal(p.cell_weights(j), ref)
+        for j, ref in enumerate(ser_cd):  # lulesh's element volumes (contracted FMA)
+            assert rel_err(p.cell_weights(j), ref) <= tol(md.loop)
 
 
 def test_batch_rejects_mixed_executors_and_kinds():
