@@ -240,8 +240,7 @@ __device__ __forceinline__ void atomic_warp(const LoopData &d, uint32_t base) {
 }
 
 template <class L, bool SOA, bool AGG>
-__global__ void __launch_bounds__(256, (65536 / (256 * L::kRegCap)) > 0 ? 65536 / (256 * L::kRegCap) : 1)
-    k_atomic(LoopData d) {
+__global__ void __launch_bounds__(256, L::kAtomicMinBlocks) k_atomic(LoopData d) {
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t base = warp * 32u; base < d.n_cells; base += n_warps * 32u)

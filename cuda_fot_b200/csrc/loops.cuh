@@ -53,6 +53,23 @@
 #define FOT_CAT2(a, b) a##b
 #define FOT_CAT(a, b) FOT_CAT2(a, b)
 #define FOT_LNS(name) FOT_CAT(name, FOT_NS_SUFFIX)
+// Resident CTAs per SM of the atomic executor, per loop (its register cap is
+// 65536 / (256 * this)); measured choices, overridable at build time.
+#ifndef FOT_ATOMIC_MINB_RES_CALC
+#define FOT_ATOMIC_MINB_RES_CALC 4
+#endif
+#ifndef FOT_ATOMIC_MINB_MINI_AERO
+#define FOT_ATOMIC_MINB_MINI_AERO 2
+#endif
+#ifndef FOT_ATOMIC_MINB_LULESH
+#define FOT_ATOMIC_MINB_LULESH 2
+#endif
+#ifndef FOT_ATOMIC_MINB_VOLNA
+#define FOT_ATOMIC_MINB_VOLNA 4
+#endif
+#ifndef FOT_ATOMIC_MINB_GETACC
+#define FOT_ATOMIC_MINB_GETACC 2
+#endif
 #define FOT_STR2(x) #x
 #define FOT_STR(x) FOT_STR2(x)
 #define FOT_FUNCTOR(file) FOT_STR(FOT_FUNCTOR_DIR/file)
@@ -78,6 +95,8 @@ struct Loop {
   static constexpr int kNumRead = 3;
   static constexpr bool kHasClass1 = true;
   static constexpr int kRegCap = 64; // registers per thread the tile kernels are held to
+  // resident 256-thread CTAs per SM the atomic executor is compiled for
+  static constexpr int kAtomicMinBlocks = FOT_ATOMIC_MINB_RES_CALC;
   // read set r: x (set 1, class 1, dim 2), q (set 2, class 0, dim 4), adt (set 3, class 0, dim 1)
   __host__ __device__ static constexpr int read_set(int r) { return r + 1; }
   __host__ __device__ static constexpr int read_class(int r) { return r == 0 ? 1 : 0; }
@@ -116,6 +135,8 @@ struct Loop {
   static constexpr int kNumRead = 1;
   static constexpr bool kHasClass1 = false;
   static constexpr int kRegCap = 128; // registers per thread the tile kernels are held to
+  // resident 256-thread CTAs per SM the atomic executor is compiled for
+  static constexpr int kAtomicMinBlocks = FOT_ATOMIC_MINB_MINI_AERO;
   __host__ __device__ static constexpr int read_set(int) { return 1; }
   __host__ __device__ static constexpr int read_class(int) { return 0; }
   __host__ __device__ static constexpr int read_dim(int) { return 28; }
@@ -164,6 +185,8 @@ struct Loop {
   static constexpr int kNumRead = 1;
   static constexpr bool kHasClass1 = false;
   static constexpr int kRegCap = 96; // registers per thread the tile kernels are held to
+  // resident 256-thread CTAs per SM the atomic executor is compiled for
+  static constexpr int kAtomicMinBlocks = FOT_ATOMIC_MINB_LULESH;
   __host__ __device__ static constexpr int read_set(int) { return 1; }
   __host__ __device__ static constexpr int read_class(int) { return 0; }
   __host__ __device__ static constexpr int read_dim(int) { return 3; }
@@ -210,6 +233,8 @@ struct Loop {
   static constexpr int kNumRead = 1;
   static constexpr bool kHasClass1 = false;
   static constexpr int kRegCap = 64; // registers per thread the tile kernels are held to
+  // resident 256-thread CTAs per SM the atomic executor is compiled for
+  static constexpr int kAtomicMinBlocks = FOT_ATOMIC_MINB_VOLNA;
   __host__ __device__ static constexpr int read_set(int) { return 1; }
   __host__ __device__ static constexpr int read_class(int) { return 0; }
   __host__ __device__ static constexpr int read_dim(int) { return 1; }
@@ -250,6 +275,8 @@ struct Loop {
   static constexpr int kNumRead = 0;
   static constexpr bool kHasClass1 = false;
   static constexpr int kRegCap = 96; // registers per thread the tile kernels are held to
+  // resident 256-thread CTAs per SM the atomic executor is compiled for
+  static constexpr int kAtomicMinBlocks = FOT_ATOMIC_MINB_GETACC;
   __host__ __device__ static constexpr int read_set(int) { return 0; }
   __host__ __device__ static constexpr int read_class(int) { return 0; }
   __host__ __device__ static constexpr int read_dim(int) { return 1; }

@@ -106,7 +106,10 @@ def test_golden_fixtures_on_gpu(name):
         order = p.cell_order()
         for j, ref in enumerate(out_cd):
             got = unpermute_cells(p.cell_weights(j), order)
-            assert bitwise_equal(got, ref), (name, j)
+            if exec_ == F().EXEC_ATOMIC:  # contracted multiply-adds
+                assert rel_err(got, ref) <= tol(md.loop), (name, j)
+            else:
+                assert bitwise_equal(got, ref), (name, j)
 
 
 def test_repeated_runs_are_deterministic_and_graph_equals_run():
