@@ -161,6 +161,8 @@ fot::HierPlanDev fot_plan::dev(uint32_t iterations) const {
   P.launch = launch.as<uint32_t>();
   P.partial = partial.ptr;
   P.comb_point = comb_point.as<uint32_t>();
+  P.tile_hdr = tile_hdr.as<uint4>();
+  P.wslot = wslot.as<uint32_t>();
   P.comb_base = comb_base.as<uint32_t>();
   P.n_slots = n_slots;
   P.n_shared = n_shared_points;

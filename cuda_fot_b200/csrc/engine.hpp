@@ -122,7 +122,7 @@ struct fot_plan {
   fot::DevBuf block_done;   // per block: completed iterations (pipelined executor)
   // split write-back kernels: two partial-sum buffers, the shared points and
   // their slot ranges, the tiles' launch order
-  fot::DevBuf partial, comb_point, comb_base, launch;
+  fot::DevBuf partial, comb_point, comb_base, launch, tile_hdr, wslot;
   uint32_t n_slots = 0, n_shared_points = 0;
   uint32_t rec_cap = 0;
   uint32_t cap[2] = {0, 0};

@@ -80,6 +80,9 @@ struct HierPlanDev {
   const uint32_t *comb_point;  // shared point g -> point number
   const uint32_t *comb_base;   // shared point g -> its slots [base[g], base[g+1])
   uint32_t n_slots, n_shared;
+  const uint4 *tile_hdr;       // per tile (launch order): start, cells | colours << 16,
+                               // written points, their offset in pts[0]
+  const uint32_t *wslot;       // per pts[0] entry: its slot, 0xFFFFFFFF private
   // per launch: tiles run (0: combine only), the buffer they fill, whether
   // the other buffer (previous iteration) is combined, CTAs doing that
   uint32_t tiles_on, put_buf, comb_on, comb_ctas;

@@ -28,9 +28,10 @@
 //   * k_hier_dsplit (direct): one CTA per tile, one thread per cell; each
 //     thread gathers its cell's rows straight from HBM/L2 through the
 //     plan-ordered mapping (like the atomic executor: thousands of
-//     independent gathers in flight per SM), computes into shared memory, and
-//     the block's sums go out as above.  Extra CTAs at the front of the grid
-//     do the combine.
+//     independent gathers in flight per SM), adds its increments into a
+//     shared-memory sum one thread colour after another, and the block's
+//     sums go out as above.  Extra CTAs at the front of the grid do the
+//     combine.
 //   * k_hier_split (staged): persistent CTAs of T compute threads and two
 //     control warps; the RECORD warp bulk-copies each tile's record (plan.cu,
 //     step 4b) into one of kRecSlots slots (TMA engine, no multicast), the
@@ -132,14 +133,23 @@ __device__ __forceinline__ void split_writeback(const LoopData &d, const HierPla
 }
 
 // Direct form: CTAs [0, comb_ctas) combine the previous buffer, the others
-// run one tile each.
+// run one tile each (hardware CTA scheduling keeps several tiles per SM in
+// different phases; a persistent form with one tile in flight per CTA and
+// the next tile's plan data prefetched measured slower).  A tile is the
+// reference's block step with HBM/L2 gathers: one thread per cell gathers its
+// rows through the plan-ordered mapping and computes its increments in
+// registers; the increments go into a zeroed shared-memory sum one thread
+// colour after another (cells of one colour write disjoint points: the
+// replay's order, bit for bit); then each written point's sum goes out (RED
+// for private points, the slot for shared ones).  The tile header (start,
+// cells | colours << 16, written points, their offset) is one 16-byte load.
 template <class L, bool SOA, int T>
 __global__ void __launch_bounds__(T, hier_min_blocks<L, T>()) k_hier_dsplit(LoopData d, HierPlanDev P) {
   using out_t = typename L::out_t;
   using read_t = typename L::read_t;
   constexpr int D = L::kDim, K = L::kOut;
   extern __shared__ __align__(16) unsigned char smem[];
-  out_t *const inc = reinterpret_cast<out_t *>(smem);
+  out_t *const acc = reinterpret_cast<out_t *>(smem);
   const uint32_t tid = threadIdx.x;
   griddep_launch_dependents();
   if (blockIdx.x < P.comb_ctas) {
@@ -151,29 +161,70 @@ __global__ void __launch_bounds__(T, hier_min_blocks<L, T>()) k_hier_dsplit(Loop
     }
     return;
   }
-  const RecView<L> m(P.rec + P.rec_off[P.launch[blockIdx.x - P.comb_ctas]]);
+  const uint4 h = __ldg(P.tile_hdr + (blockIdx.x - P.comb_ctas));
+  const uint32_t start = h.x, ncell = h.y & 0xFFFFu, ntcol = h.y >> 16, n0 = h.z, poff = h.w;
+  for (uint32_t e = tid; e < n0 * K; e += T) acc[e] = out_t(0);
+  // this thread's first written point (issued early; used after the sums)
+  uint32_t p_first = 0, ws_first = 0;
+  if (tid < n0) {
+    p_first = __ldg(P.pts[0] + poff + tid);
+    ws_first = __ldg(P.wslot + poff + tid);
+  }
   if constexpr (L::kWritesCell) griddep_wait();  // the previous iteration may still write cell data
-  if (tid < m.ncell) {
-    const uint32_t pos = m.start + tid;
+  const bool active = tid < ncell;
+  const uint32_t pos = start + tid;
+  uint32_t my_col = 0xFFFFFFFFu;
+  uint16_t l0[D];
+  out_t v[D][K];
+  if (active) {
     GlobalRows<L, SOA> rows;
     load_row<D>(d.map[0], pos, rows.p[0]);
     if constexpr (L::kHasClass1) load_row<D>(d.map[1], pos, rows.p[1]);
+#pragma unroll
+    for (int q = 0; q < D; ++q) l0[q] = __ldg(P.lidx[0] + (size_t)q * d.n_cells + pos);
+    my_col = __ldg(P.tcol + pos);
     static_for_read<L>([&](auto r) {
       constexpr int R = decltype(r)::value;
       rows.base[R] = static_cast<const read_t *>(d.point[L::read_set(R)]);
       rows.np[R] = d.n_points[L::read_set(R)];
     });
-    out_t v[D][K];
     Direct dir{d.cell, pos, d.n_cells};
     L::cell(rows, dir, v);
-#pragma unroll
-    for (int q = 0; q < D; ++q)
-#pragma unroll
-      for (int k = 0; k < K; ++k) inc[(k * D + q) * T + tid] = v[q][k];
   }
-  __syncthreads();
+  __syncthreads();  // the sums are zeroed
+  for (uint32_t col = 0; col < ntcol; ++col) {
+    if (my_col == col) {
+#pragma unroll
+      for (int q = 0; q < D; ++q)
+#pragma unroll
+        for (int k = 0; k < K; ++k) acc[(uint32_t)l0[q] * K + k] += v[q][k];
+    }
+    __syncthreads();
+  }
   if constexpr (!L::kWritesCell) griddep_wait();  // the previous iteration's writes are visible
-  split_writeback<L, SOA, T>(d, P, m, inc, tid);
+  out_t *out = static_cast<out_t *>(d.out);
+  out_t *put = static_cast<out_t *>(P.partial) + (size_t)P.put_buf * P.n_slots * K;
+  for (uint32_t j = tid; j < n0; j += T) {
+    const uint32_t p = j == tid ? p_first : __ldg(P.pts[0] + poff + j);
+    const uint32_t ws = j == tid ? ws_first : __ldg(P.wslot + poff + j);
+    const out_t *a = acc + (size_t)j * K;
+    if (ws == 0xFFFFFFFFu) {
+      // private point: this block alone writes it in this iteration
+      if constexpr (sizeof(out_t) == 8) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) atomicAdd(out + out_index(SOA, d.n_points[0], p, K, k), a[k]);
+      } else {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          out_t *o = out + out_index(SOA, d.n_points[0], p, K, k);
+          __stcg(o, __ldcg(o) + a[k]);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < K; ++k) __stcg(put + (size_t)ws * K + k, a[k]);
+    }
+  }
 }
 
 template <class L, bool SOA, int T, uint32_t kRecSlots>

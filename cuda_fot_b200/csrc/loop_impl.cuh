@@ -169,9 +169,9 @@ void smem_layout(uint32_t cap0, uint32_t cap1, uint32_t variant, uint32_t rec_ca
   SmemLayout s;
   size_t off = 0;
   if ((variant & kVariantSplit) && !(variant & kVariantPipe)) {
-    // direct split write-back: the per-slot increments only
-    s.inc_off = 0;
-    s.total = a16((size_t)L::kOut * L::kDim * threads * sizeof(out_t));
+    // direct split write-back: the block's sums only
+    s.acc_off = 0;
+    s.total = a16((size_t)cap0 * L::kOut * sizeof(out_t));
     *out = s;
     return;
   }

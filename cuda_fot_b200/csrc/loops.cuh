@@ -65,7 +65,7 @@
 #define FOT_ATOMIC_MINB_LULESH 2
 #endif
 #ifndef FOT_ATOMIC_MINB_VOLNA
-#define FOT_ATOMIC_MINB_VOLNA 4
+#define FOT_ATOMIC_MINB_VOLNA 8
 #endif
 #ifndef FOT_ATOMIC_MINB_GETACC
 #define FOT_ATOMIC_MINB_GETACC 2

@@ -736,6 +736,17 @@ int build_hier_plan(fot_problem *p, fot_plan *plan) {
       FOT_TRY(upload(plan->comb_point, sr.point));
       FOT_TRY(upload(plan->comb_base, sr.base));
       FOT_TRY(upload(plan->launch, final_of));
+      FOT_TRY(upload(plan->wslot, sr.wslot));
+      // direct form: one 16-byte header per tile, in launch order
+      std::vector<uint32_t> hdr((size_t)4 * nfb);
+      for (uint32_t t = 0; t < nfb; ++t) {
+        const uint32_t b = final_of[t], fb = order[b];
+        hdr[4 * t + 0] = block_start[b];
+        hdr[4 * t + 1] = (block_start[b + 1] - block_start[b]) | ((uint32_t)h_ntcol[fb] << 16);
+        hdr[4 * t + 2] = h_off[0][b + 1] - h_off[0][b];
+        hdr[4 * t + 3] = h_off[0][b];
+      }
+      FOT_TRY(upload(plan->tile_hdr, hdr));
       plan->n_slots = sr.n_slots;
       plan->n_shared_points = (uint32_t)sr.point.size();
     }
