@@ -12,7 +12,9 @@ best (regret) and with a fixed default plan (what the model gains).
 
 Features (FEATURES below): mesh size and bytes, the loop kind, the histogram
 of point degrees, the bandwidth and mean cell span of the ordered mapping,
-and the plan descriptor.
+the sectors per cell of the reference's sector model in the candidate's point
+layout (warps of 32 cells), and the plan descriptor.  The ordering-dependent
+ones are computed on the GPU from the mappings alone (ordering_stats).
 """
 from __future__ import annotations
 
@@ -36,7 +38,7 @@ DEFAULT_MODEL = os.path.join(MODEL_DIR, "costmodel.npz")
 DEFAULT_CORPUS = os.path.join(MODEL_DIR, "corpus.npz")
 
 FEATURES = [
-    "log10_cells", "log10_points", "mesh_dim", "log10_unique_bytes",
+    "log10_cells", "log10_points", "log2_1p_sectors_per_cell", "log10_unique_bytes",
     "read_bytes_per_cell/100", "direct_bytes_per_cell/100",
     "loop_res_calc", "loop_mini_aero", "loop_lulesh", "loop_volna", "loop_getacc",
     "deg_le2", "deg_3_4", "deg_5_6", "deg_ge7",
@@ -49,14 +51,13 @@ assert len(FEATURES) == N_FEATURES
 _lib = F._lib
 _fp = C.POINTER(C.c_float)
 
+SECTOR_CELLS = 32  # sectors are counted per warp-sized run of cells
 
-def mesh_features(md: mg.MeshData) -> np.ndarray:
-    """16 features of a mesh in its current numbering (the loop's output
-    dimension is implied by the loop's one-hot)."""
-    m0 = np.asarray(md.maps[0])
-    n, dim = m0.shape
-    np0 = md.n_points[0]
+
+def static_features(md: mg.MeshData) -> dict:
+    """Ordering-independent properties of a mesh."""
     info = F.loop_info(md.loop)
+    dim = int(np.asarray(md.maps[0]).shape[1])
     read_bytes = 0
     if md.loop == mg.RES_CALC:
         read_bytes = dim * (2 * 8 + 4 * 8 + 8)
@@ -67,21 +68,53 @@ def mesh_features(md: mg.MeshData) -> np.ndarray:
     elif md.loop == mg.VOLNA:
         read_bytes = dim * 4
     direct = sum(info.cell_dim[j] * info.cell_type_size[j] for j in range(info.n_cell_sets))
-    deg = np.bincount(m0.ravel(), minlength=np0)
-    hist = np.array([(deg <= 2).mean(), ((deg >= 3) & (deg <= 4)).mean(),
-                     ((deg >= 5) & (deg <= 6)).mean(), (deg >= 7).mean()])
-    span = (m0.max(axis=1).astype(np.int64) - m0.min(axis=1).astype(np.int64))
+    return {"loop": md.loop, "n_cells": int(md.n_cells), "n_points": int(md.n_points[0]),
+            "unique_bytes": int(md.unique_bytes()), "read_bytes": read_bytes, "direct_bytes": direct}
+
+
+def ordered_stats(p: "F.Problem") -> dict:
+    """Ordering-dependent statistics of a problem in its current numbering,
+    computed on the GPU (fot_mesh_features, fot_sector_count): nothing but
+    the totals leaves the device."""
+    f = p.mesh_features()
+    sa, _ = p.sector_count(SECTOR_CELLS, "aos")
+    ss, _ = p.sector_count(SECTOR_CELLS, "soa")
+    f["sectors_per_cell"] = {"aos": sa / p.n_cells, "soa": ss / p.n_cells}
+    return f
+
+
+def light_problem(md: mg.MeshData) -> "F.Problem":
+    """A problem holding only the mesh's mappings (datasets zero): enough to
+    apply orderings and partitions and take ordered_stats on the GPU."""
+    return F.Problem(md.loop, md.n_cells, md.n_points, md.maps, "aos")
+
+
+def ordering_stats(md: mg.MeshData, order, part: int) -> dict:
+    """ordered_stats of md after an ordering and partition, all on the GPU."""
+    p = light_problem(md)
+    if order is not None:
+        p.reorder(T.ORDERS[order], seed=1)
+    if part:
+        p.partition(part)
+        p.reorder_to_partition()
+        p.renumber_points()
+    return ordered_stats(p)
+
+
+def mesh_features(st: dict, stats: dict, layout: str) -> np.ndarray:
+    """16 mesh features of an ordered mesh for a point layout."""
     onehot = np.zeros(5)
-    onehot[md.loop] = 1
+    onehot[st["loop"]] = 1
     f = np.concatenate([
-        [np.log10(n), np.log10(np0), dim, np.log10(md.unique_bytes()),
-         read_bytes / 100.0, direct / 100.0], onehot, hist,
-        [np.log10(1 + span.max()), np.log10(1 + span.mean())]])
+        [np.log10(st["n_cells"]), np.log10(st["n_points"]),
+         np.log2(1.0 + stats["sectors_per_cell"][layout]), np.log10(st["unique_bytes"]),
+         st["read_bytes"] / 100.0, st["direct_bytes"] / 100.0], onehot, stats["deg_hist"],
+        [np.log10(1 + stats["span_max"]), np.log10(1 + stats["span_mean"])]])
     return f.astype(np.float32)
 
 
 def plan_features(c: T.Candidate) -> np.ndarray:
-    """8 plan features; the seventh is 1 for direct (unstaged) reads of a
+    """8 plan features; the seventh is 1 for the direct (unstaged) form of a
     hierarchical plan and for an atomic plan without warp aggregation, the
     last 1 for SOA point data."""
     ex = np.zeros(3)
@@ -94,8 +127,8 @@ def plan_features(c: T.Candidate) -> np.ndarray:
                                 1.0 if c.layout == "soa" else 0.0]]).astype(np.float32)
 
 
-def features(mesh_f: np.ndarray, c: T.Candidate) -> np.ndarray:
-    return np.concatenate([mesh_f, plan_features(c)]).astype(np.float32)
+def features(st: dict, stats: dict, c: T.Candidate) -> np.ndarray:
+    return np.concatenate([mesh_features(st, stats, c.layout), plan_features(c)]).astype(np.float32)
 
 
 # ---------------------------------------------------------------------------
@@ -199,15 +232,8 @@ def load_default() -> Optional[CostModel]:
 # ---------------------------------------------------------------------------
 def corpus_candidates(loop: int) -> List[T.Candidate]:
     """Plan candidates of one (mesh, ordering): point layouts x executors x
-    block sizes x staging; partitioned variants are separate orderings."""
-    out = []
-    for lay in ("aos", "soa"):
-        out.append(T.Candidate(None, 0, "atomic", 256, layout=lay))
-        out.append(T.Candidate(None, 0, "atomic", 256, aggregate=False, layout=lay))
-        for b in (128, 256, 512):
-            out.append(T.Candidate(None, 0, "hier", b, False, layout=lay))
-        out.append(T.Candidate(None, 0, "hier", 128, True, layout=lay))
-    return out
+    block sizes x kernel form; partitioned variants are separate orderings."""
+    return T.plan_candidates(None, 0)
 
 
 ORDERINGS = [(None, 0), ("random", 0), ("rcm", 0), ("gps", 0), ("gps", 128), ("gps", 256),
@@ -238,9 +264,10 @@ def generate(loops: Sequence[int], sizes: Sequence[float], seeds: Sequence[int],
     """Time every (mesh, ordering, plan) and store features and log times.
 
     Per mesh group the info records the wall time of its exhaustive sweep
-    (orderings, plan builds and timings) and of its orderings alone: the
-    model's pick needs the orderings (its features are those of the ordered
-    mesh) but no plan build or timing, which is the tuning time it saves."""
+    (orderings with the datasets, plan builds and timings) and of what the
+    model's pick needs instead: every ordering applied to the mappings alone
+    and its statistics taken on the GPU (pick_s) -- no plan build, no timing
+    and no ordered copy of the datasets."""
     X, y, group, labels, secs_all = [], [], [], [], []
     info = []
     t_start = time.time()
@@ -250,25 +277,22 @@ def generate(loops: Sequence[int], sizes: Sequence[float], seeds: Sequence[int],
             for size in sizes:
                 if time.time() - t_start > time_limit_s:
                     break
-                t_group = time.time()
                 md = mesh_for(loop, size, seed)
+                t_group = time.time()
+                st = static_features(md)
+                # what the model's pick needs: every ordering's statistics,
+                # computed on the GPU from the mappings alone
+                t_p = time.time()
+                stats = {op: ordering_stats(md, *op) for op in ORDERINGS}
+                pick_s = time.time() - t_p
                 cache = T.OrderedCache(md)
                 orders_s = 0.0
                 n0 = len(y)
                 for order, part in ORDERINGS:
                     t_o = time.time()
-                    mdo = cache.get(order, part)
-                    mf = mesh_features(mdo)
+                    cache.get(order, part)
                     orders_s += time.time() - t_o
-                    for c in corpus_candidates(loop):
-                        if part:
-                            # blocks follow the parts: block size = part size
-                            if c.exec != "atomic" and c.block != 256:
-                                continue
-                            blk = 256 if c.exec == "atomic" else part
-                            c = T.Candidate(order, part, c.exec, blk, c.direct, c.aggregate, c.layout)
-                        else:
-                            c = T.Candidate(order, 0, c.exec, c.block, c.direct, c.aggregate, c.layout)
+                    for c in T.plan_candidates(order, part):
                         try:
                             p, plan = T.build(cache.get(order, part, c.layout), c)
                             t1 = T.time_plan(p, plan, iters=2, warmup=1)
@@ -277,7 +301,7 @@ def generate(loops: Sequence[int], sizes: Sequence[float], seeds: Sequence[int],
                             del plan, p
                         except F.FotError:
                             continue
-                        X.append(features(mf, c))
+                        X.append(features(st, stats[(order, part)], c))
                         y.append(np.log(secs))
                         secs_all.append(secs)
                         group.append(gid)
@@ -285,11 +309,12 @@ def generate(loops: Sequence[int], sizes: Sequence[float], seeds: Sequence[int],
                 sweep_s = time.time() - t_group
                 info.append({"gid": gid, "loop": int(loop), "cells": int(md.n_cells), "seed": int(seed),
                              "size": float(size), "samples": len(y) - n0,
-                             "sweep_s": round(sweep_s, 3), "orders_s": round(orders_s, 3)})
+                             "sweep_s": round(sweep_s - pick_s, 3), "orders_s": round(orders_s, 3),
+                             "pick_s": round(pick_s, 3)})
                 if verbose:
                     print(f"  {mg.LOOP_NAMES[loop]} {md.n_cells} seed {seed}: {len(y) - n0} samples, "
-                          f"sweep {sweep_s:.1f}s (orderings {orders_s:.1f}s), total {len(y)} samples, "
-                          f"{time.time()-t_start:.0f}s", flush=True)
+                          f"sweep {sweep_s - pick_s:.1f}s (orderings {orders_s:.1f}s), model inputs "
+                          f"{pick_s:.1f}s, total {len(y)} samples, {time.time()-t_start:.0f}s", flush=True)
                 gid += 1
                 del cache
     data = {"X": np.array(X, np.float32), "y": np.array(y, np.float32),
@@ -356,16 +381,19 @@ def evaluate(model: CostModel, data: dict, mask: np.ndarray) -> dict:
 
 
 def pick(model: CostModel, md: mg.MeshData, candidates: List[T.Candidate]) -> T.Candidate:
-    """The candidate with the smallest predicted time (orderings are applied
-    to compute the ordered-mesh features)."""
-    cache = T.OrderedCache(md)
-    rows, cands = [], []
+    """The candidate with the smallest predicted time.  Each distinct
+    ordering is applied to a problem holding only the mesh's mappings and its
+    statistics are taken on the GPU (ordering_stats); nothing is timed."""
+    st = static_features(md)
+    stats = {}
+    rows = []
     for c in candidates:
-        mf = mesh_features(cache.get(c.order, c.partition))
-        rows.append(features(mf, c))
-        cands.append(c)
+        key = (c.order, c.partition)
+        if key not in stats:
+            stats[key] = ordering_stats(md, *key)
+        rows.append(features(st, stats[key], c))
     pred = model.predict(np.array(rows))
-    return cands[int(np.argmin(pred))]
+    return candidates[int(np.argmin(pred))]
 
 
 # ---------------------------------------------------------------------------
@@ -404,10 +432,10 @@ def train_and_evaluate(data: dict, holdout_seed: Optional[int] = None, epochs: i
     ev = evaluate(m, data, ~train)
     held = [d for d in info if d["seed"] == hold]
     sweep_s = sum(d.get("sweep_s", 0.0) for d in held)
-    orders_s = sum(d.get("orders_s", 0.0) for d in held)
+    orders_s = sum(d.get("pick_s", d.get("orders_s", 0.0)) for d in held)
     ev.update({"holdout_seed": hold, "train_rows": int(train.sum()), "test_rows": int((~train).sum()),
                "final_loss": float(losses[-1]), "train_s": round(train_s, 2),
-               "heldout_sweep_s": round(sweep_s, 1), "heldout_orderings_s": round(orders_s, 1),
+               "heldout_sweep_s": round(sweep_s, 1), "heldout_model_inputs_s": round(orders_s, 1),
                "tuning_time_saved_frac": (1.0 - orders_s / sweep_s) if sweep_s > 0 else None})
     return m, ev
 

@@ -153,6 +153,14 @@ class Plan:
     def graph(self, iterations: int, stream=None) -> "Graph":
         return Graph(self, iterations, stream)
 
+    def sector_count(self, layout: Optional[str] = None):
+        """The reference's sector model over this plan's blocks and their
+        written points (fot_plan_sector_count): (sectors, blocks)."""
+        lay = -1 if layout is None else (SOA if layout == "soa" else AOS)
+        sec, nb = C.c_uint64(), C.c_uint64()
+        _check(_lib.fot_plan_sector_count(self._h, C.c_int(lay), C.byref(sec), C.byref(nb)))
+        return sec.value, nb.value
+
     def inject_lost_flag(self, block: int) -> None:
         """Test hook (fot_plan_inject_lost_flag): lose one block's completion
         flag so that the next run's dependency waits hit their time limit."""
@@ -300,6 +308,23 @@ class Problem:
                            [self.point_weights(k) for k in range(self.info.n_point_sets)],
                            [self.cell_weights(j) for j in range(self.info.n_cell_sets)],
                            self.layout)
+
+    # ---- statistics (GPU) ----------------------------------------------------------
+    def mesh_features(self) -> dict:
+        """fot_mesh_features: spread of mapping 0's rows and point degrees."""
+        out = (C.c_double * 6)()
+        _check(_lib.fot_mesh_features(self._h, out, C.c_int(6)))
+        return {"span_max": out[0], "span_mean": out[1],
+                "deg_hist": [out[2], out[3], out[4], out[5]]}
+
+    def sector_count(self, cells_per_block: int = 256, layout: Optional[str] = None):
+        """The reference's sector model over runs of cells_per_block cells
+        (fot_sector_count): (sectors, blocks)."""
+        lay = -1 if layout is None else (SOA if layout == "soa" else AOS)
+        sec, nb = C.c_uint64(), C.c_uint64()
+        _check(_lib.fot_sector_count(self._h, C.c_uint32(cells_per_block), C.c_int(lay),
+                                     C.byref(sec), C.byref(nb)))
+        return sec.value, nb.value
 
     # ---- orderings (problem.hpp:439-551) ----------------------------------------
     def reorder(self, order: int = ORDER_GPS, seed: int = 1) -> None:

@@ -7,7 +7,9 @@ A candidate is (ordering, partition size, executor, block size, layout):
 * partition -- 0, or the part size of fot_partition followed by
   fot_reorder_to_partition and fot_renumber_points (the reference's
   partition -> reorderToPartition -> renumberPoints sequence);
-* executor  -- "atomic", "hier" (persistent) or "hier_launch";
+* executor  -- "atomic", "hier" (persistent; split write-back kernel,
+  staged or -- with direct -- gathering rows straight from HBM/L2) or
+  "hier_launch";
 * block     -- cells per block (hierarchical) / threads per CTA (atomic);
 * layout    -- "aos" or "soa" point data (the reference's Problem<SOA>).
 
@@ -50,22 +52,36 @@ class Candidate:
         return f"{o}{p}/{self.exec}{d}{a}/{self.block}{lay}"
 
 
-def default_candidates(loop: int, quick: bool = False) -> List[Candidate]:
-    orders = ["gps", "rcm"] if quick else [None, "random", "rcm", "gps"]
-    blocks = [128, 256] if quick else [128, 256, 512]
+def plan_candidates(order: Optional[str], part: int) -> List[Candidate]:
+    """The plans of one (ordering, partition): for both point layouts, the
+    atomic executor with and without warp aggregation and the hierarchical
+    executor's staged and direct split write-back kernels (blocks of 128, 256,
+    512 and 128, 256 cells; on a partition, blocks of the part size)."""
     out = []
     for lay in ("aos", "soa"):
-        for o in orders:
-            out.append(Candidate(o, 0, "atomic", 256, layout=lay))
-            out.append(Candidate(o, 0, "atomic", 256, aggregate=False, layout=lay))
-            if not quick:
-                out.append(Candidate(o, 0, "hier", 128, True, layout=lay))
-            for b in blocks:
-                out.append(Candidate(o, 0, "hier", b, layout=lay))
-        if not quick:
-            for b in blocks:
-                out.append(Candidate("gps", b, "hier", b, layout=lay))
-                out.append(Candidate("rcm", b, "hier", b, layout=lay))
+        out.append(Candidate(order, part, "atomic", 256, layout=lay))
+        out.append(Candidate(order, part, "atomic", 256, aggregate=False, layout=lay))
+        if part:
+            out.append(Candidate(order, part, "hier", part, layout=lay))
+            out.append(Candidate(order, part, "hier", part, True, layout=lay))
+            continue
+        for b in (128, 256, 512):
+            out.append(Candidate(order, 0, "hier", b, layout=lay))
+        for b in (128, 256):
+            out.append(Candidate(order, 0, "hier", b, True, layout=lay))
+    return out
+
+
+def default_candidates(loop: int, quick: bool = False) -> List[Candidate]:
+    """The sweep: plan_candidates over the orderings (quick: RCM and GPS, and
+    RCM with parts of 256 cells; else also the given numbering, a random one
+    and GPS with parts of 128, 256 and 512)."""
+    orderings = [("gps", 0), ("rcm", 0), ("rcm", 256)] if quick else \
+        [(None, 0), ("random", 0), ("rcm", 0), ("gps", 0), ("gps", 128), ("gps", 256),
+         ("rcm", 256), ("gps", 512)]
+    out = []
+    for o, part in orderings:
+        out.extend(plan_candidates(o, part))
     return out
 
 

@@ -269,6 +269,30 @@ int fot_batch_run(fot_batch *b, uint32_t iterations, void *stream);
 int fot_batch_sync(fot_batch *b, void *stream);
 int fot_batch_destroy(fot_batch *b);
 
+/* ---- mesh statistics: the sector model and the cost model's mesh features - */
+
+/* Statistics of mapping 0 in the problem's CURRENT numbering, on the GPU:
+ * out[0] the largest and out[1] the mean spread (max - min point number) of a
+ * cell's row; out[2..5] the fractions of points of degree <= 2, 3-4, 5-6 and
+ * >= 7.  n_out >= FOT_MESH_FEATURES.  No counterpart in the reference (its
+ * orderings report bandwidth on the host, reorder.hpp). */
+#define FOT_MESH_FEATURES 6
+int fot_mesh_features(fot_problem *p, double *out, int n_out);
+
+/* The reference's sector model, countCacheLinesForBlock (problem.hpp:654-672)
+ * as its global-colouring loop applies it (problem.hpp:145-152): for blocks of
+ * `cells_per_block` consecutive cells (current order), the distinct 32-byte
+ * sectors of point dataset 0 that their points touch -- AOS: every element
+ * of every row; SOA: distinct p / (32 / type size), times the dimension --
+ * summed over the blocks.  layout: FOT_AOS, FOT_SOA, or -1 for the problem's.
+ * The reference prints sectors * 32 * 2 per iteration as its "cache line"
+ * bandwidth (problem.hpp:191-192). */
+int fot_sector_count(fot_problem *p, uint32_t cells_per_block, int layout, uint64_t *sectors,
+                     uint64_t *blocks);
+/* The same over a hierarchical plan's blocks and their written points, as
+ * loopGPUHierarchical applies it to points_to_be_cached (problem.hpp:233-240). */
+int fot_plan_sector_count(const fot_plan *plan, int layout, uint64_t *sectors, uint64_t *blocks);
+
 /* ---- the learned plan cost model ------------------------------------------- */
 
 /* A 24 -> 64 -> 64 -> 1 ReLU MLP (FP32) predicting log(seconds per

@@ -68,6 +68,7 @@ def ref():
         lib.ref_loop_serial.restype = C.c_int
         lib.ref_loop_omp.restype = C.c_int
         lib.ref_hier_plan.restype = C.c_int
+        lib.ref_count_cache_lines.restype = C.c_uint64
         _ref = lib
     return _ref
 
@@ -222,3 +223,32 @@ def ref_hier_plan(md, block_size: int):
         raise RuntimeError(f"ref_hier_plan failed: {rc}")
     return {"seconds": secs.value, "n_colours": nc.value, "n_blocks": nb.value,
             "avg_thread_colours": tc.value}
+
+
+def sector_count(map0: np.ndarray, cells_per_block: int, dim: int, type_size: int, soa: bool) -> int:
+    """The reference's sector model (countCacheLinesForBlock,
+    problem.hpp:654-672) summed over blocks of consecutive cells, restated
+    with numpy: per block, the distinct 32-byte sectors of point dataset 0
+    touched -- AOS: element p * dim + d lies in sector (p * dim + d) //
+    (32 // type_size); SOA: distinct p // (32 // type_size), times dim."""
+    m = np.asarray(map0, dtype=np.int64)
+    per = 32 // type_size
+    total = 0
+    for c0 in range(0, m.shape[0], cells_per_block):
+        pts = m[c0:c0 + cells_per_block].ravel()
+        if soa:
+            total += dim * len(np.unique(pts // per))
+        else:
+            el = (pts[:, None] * dim + np.arange(dim)[None, :]).ravel()
+            total += len(np.unique(el // per))
+    return int(total)
+
+
+def ref_sector_count(map0: np.ndarray, cells_per_block: int, dim: int, type_size: int,
+                     soa: bool) -> int:
+    """The same through the reference's own countCacheLinesForBlock."""
+    m = np.ascontiguousarray(map0, dtype=np.uint32)
+    return int(ref().ref_count_cache_lines(m.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                           C.c_uint32(m.shape[0]), C.c_uint32(m.shape[1]),
+                                           C.c_uint32(cells_per_block), C.c_uint32(dim),
+                                           C.c_uint32(type_size), C.c_int(int(soa))))

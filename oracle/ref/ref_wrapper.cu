@@ -11,9 +11,11 @@
  *   Problem<SOA>::loopCPUCellCentredOMP<StepOMP>  problem.hpp:405-437
  *   Mesh::colourCells                              mesh.hpp:117-162
  *   HierarchicalColourMemory<SOA>                  colouring.hpp:44-147
+ *   countCacheLinesForBlock<SOA>                   problem.hpp:654-672
  * with the data bindings of each driver's initProblem (res_calc.cu:10-28,
  * mini_aero.cu:10-24, lulesh.cu:10-24, volna.cu:11-27, getacc.cu:11-26).
  */
+#include <algorithm>
 #include <chrono>
 #include <cstdint>
 #include <cstring>
@@ -227,6 +229,22 @@ int ref_hier_plan(int loop, uint32_t n_cells, const uint32_t *n_points,
   if (avg_thread_colours) *avg_thread_colours = nb ? tc / nb : 0.0;
   delete p;
   return 0;
+}
+
+/* The reference's sector model (countCacheLinesForBlock, problem.hpp:654-672)
+ * summed over blocks of cells_per_block consecutive cells of a mapping, as
+ * loopGPUCellCentred applies it to a colour's cell list (problem.hpp:145-152):
+ * `dim` and `type_size` describe point dataset 0. */
+uint64_t ref_count_cache_lines(const uint32_t *map, uint32_t n_cells, uint32_t mesh_dim,
+                               uint32_t cells_per_block, uint32_t dim, uint32_t type_size, int soa) {
+  uint64_t total = 0;
+  for (uint32_t c0 = 0; c0 < n_cells; c0 += cells_per_block) {
+    const uint32_t c1 = std::min<uint32_t>(n_cells, c0 + cells_per_block);
+    const uint32_t *b = map + (size_t)mesh_dim * c0, *e = map + (size_t)mesh_dim * c1;
+    total += soa ? countCacheLinesForBlock<true>(b, e, dim, type_size)
+                 : countCacheLinesForBlock<false>(b, e, dim, type_size);
+  }
+  return total;
 }
 
 } // extern "C"

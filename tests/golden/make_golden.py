@@ -5,7 +5,8 @@ and the outputs of the REFERENCE'S OWN serial loop on them
 (``Problem::loopCPUCellCentred<StepSeq>``, problem.hpp:362-380), compiled from
 the reference sources by ``make -C oracle ref`` into oracle/_ref/libref.so.
 The fixtures pin the oracle (tests/test_oracle.py) and, through it, the GPU
-executors.  Run from the repository root where the reference sources exist:
+executors; sectors.json holds the reference's own sector model
+(countCacheLinesForBlock, problem.hpp:654-672) on the same meshes.  Run from the repository root where the reference sources exist:
 
     python tests/golden/make_golden.py
 """
@@ -38,6 +39,31 @@ def fixture_name(loop, layout):
     return f"{mg.LOOP_NAMES[loop]}_{layout}.npz"
 
 
+SECTOR_BLOCKS = (32, 256)
+
+
+def sector_fixtures(here):
+    """sectors.json: the reference's own sector model (countCacheLinesForBlock
+    over blocks of consecutive cells) on the fixture meshes, both layouts."""
+    import json
+    out = []
+    for loop, kw, layout in CASES:
+        if layout != "aos":
+            continue
+        md = mg.GENERATORS[loop](seed=1, layout=layout, **kw)
+        dim = md.point_data[0].shape[1]
+        ts = md.point_data[0].dtype.itemsize
+        for soa in (False, True):
+            for b in SECTOR_BLOCKS:
+                out.append({"loop": mg.LOOP_NAMES[loop], "kwargs": kw, "cells_per_block": b,
+                            "soa": soa, "dim": dim, "type_size": ts,
+                            "sectors": O.ref_sector_count(md.maps[0], b, dim, ts, soa)})
+    path = os.path.join(here, "sectors.json")
+    with open(path, "w") as f:
+        json.dump(out, f, indent=1)
+    print(path, len(out), "sector cases")
+
+
 def main():
     O.build_ref()
     here = os.path.dirname(os.path.abspath(__file__))
@@ -58,6 +84,7 @@ def main():
         path = os.path.join(here, fixture_name(loop, layout))
         np.savez_compressed(path, **arrays)
         print(path, md.n_cells, "cells")
+    sector_fixtures(here)
 
 
 if __name__ == "__main__":

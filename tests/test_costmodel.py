@@ -33,12 +33,22 @@ def test_features_shape_and_content():
     from cuda_fot_b200 import meshgen as mg
     from cuda_fot_b200 import tune as T
     md = mg.res_calc(30, 20)
-    mf = CM.mesh_features(md)
-    f = CM.features(mf, T.Candidate("gps", 0, "hier", 256, True))
+    st = CM.static_features(md)
+    assert st["n_cells"] == md.n_cells and st["unique_bytes"] == md.unique_bytes()
+    # the ordering-dependent statistics come from the GPU (ordering_stats);
+    # here a stand-in with the same keys
+    stats = {"span_max": 63.0, "span_mean": 7.0, "deg_hist": [0.1, 0.2, 0.3, 0.4],
+             "sectors_per_cell": {"aos": 1.0, "soa": 3.0}}
+    f = CM.features(st, stats, T.Candidate("gps", 0, "hier", 256, True))
     assert f.shape == (CM.N_FEATURES,) and np.all(np.isfinite(f))
     assert f[CM.FEATURES.index("loop_res_calc")] == 1
     assert f[CM.FEATURES.index("exec_hier")] == 1 and f[CM.FEATURES.index("direct_reads_or_plain_atomics")] == 1
     assert abs(f[CM.FEATURES.index("log2_block")] - 8) < 1e-6
+    assert abs(f[CM.FEATURES.index("log2_1p_sectors_per_cell")] - 1.0) < 1e-6
+    assert abs(f[CM.FEATURES.index("log10_1p_bandwidth")] - np.log10(64.0)) < 1e-6
+    f_soa = CM.features(st, stats, T.Candidate("gps", 0, "hier", 256, True, layout="soa"))
+    assert abs(f_soa[CM.FEATURES.index("log2_1p_sectors_per_cell")] - 2.0) < 1e-6
+    assert f_soa[CM.FEATURES.index("soa_layout")] == 1
 
 
 def _dataset(n=512, seed=3):

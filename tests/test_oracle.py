@@ -107,3 +107,21 @@ def test_is_permutation():
     assert O.is_permutation(np.array([2, 0, 1]))
     assert not O.is_permutation(np.array([2, 0, 2]))
     assert not O.is_permutation(np.array([3, 0, 1]))
+
+
+def _sector_cases():
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "sectors.json")) as f:
+        return json.load(f)
+
+
+def test_sector_model_matches_the_reference():
+    """The numpy restatement of the reference's sector model
+    (countCacheLinesForBlock) equals the reference's own counts on the
+    fixture meshes (tests/golden/sectors.json), both layouts, two block
+    sizes."""
+    for c in _sector_cases():
+        md = mg.GENERATORS[mg.LOOP_NAMES.index(c["loop"])](seed=1, **c["kwargs"])
+        got = O.sector_count(md.maps[0], c["cells_per_block"], c["dim"], c["type_size"], c["soa"])
+        assert got == c["sectors"], c
