@@ -17,6 +17,12 @@ mapping once.
 Multi-GPU: the loop is single-GPU (the engine does not shard a mesh), so N
 GPUs run N independent replicas ("scaling": "weak"); value = the bytes all
 ranks processed / the max over ranks of the timed region.
+
+At N=1 the line also carries the other configurations under their own keys
+(cuda_fot_b200/bench_configs.py): res_calc 1000^2 with an L2-flushed timing,
+LULESH 96^3 before and after reordering, the 512-mesh batch, the cost
+model's held-out regret, the atomic executor's run-to-run spread and the
+plan-build times; --no-extras skips them.
 """
 from __future__ import annotations
 
@@ -237,6 +243,9 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the other configurations (res_calc 1000^2, LULESH 96^3, the 512-mesh "
+                         "batch, the cost model's held-out regret, the atomic spread, plan builds)")
     ap.add_argument("--plan", default=None,
                     help="force a plan by its label, order[+partN]/exec[d][-plain]/block[@soa], "
                          "e.g. rcm/atomic-plain/256@soa")
@@ -249,6 +258,7 @@ def main(argv=None):
     import torch
     rank, world, local = dist_setup(args.gpus)
     from cuda_fot_b200 import fot as F
+    from cuda_fot_b200 import meshgen as mg
     from cuda_fot_b200 import tune as T
 
     md = make_workload(args)
@@ -281,12 +291,13 @@ def main(argv=None):
         choice_src = "forced"
     sweep_res = []
     if choice_src != "forced":
-        cands = T.default_candidates(md.loop, quick=True)
+        # the exhaustive measured sweep over the same candidates the model
+        # picks from: the fallback, and the judge of the model's pick
+        cands = T.default_candidates(md.loop)
         if chosen is not None and chosen.label() not in [c.label() for c in cands]:
             cands.append(chosen)
         t_sweep = time.perf_counter()
-        for c in cands:
-            sweep_res.append(T.measure(cache, c, iters=5, warmup=3))
+        sweep_res = T.sweep(md, cands, iters=5, warmup=3, cache=cache)
         sweep_s = time.perf_counter() - t_sweep
         if chosen is None:
             chosen = T.best(sweep_res)["cand"]
@@ -296,10 +307,19 @@ def main(argv=None):
     md_run = cache.get(chosen.order, chosen.partition, chosen.layout)
     p, plan = T.build(md_run, chosen)
     # launches of one Plan.run(K) call: the atomic executor launches once per
-    # iteration, the persistent hierarchical kernel once per call, the
-    # per-colour form once per colour and iteration
+    # iteration; the split write-back kernels once per iteration plus one
+    # combine-only launch when blocks share points; the other persistent
+    # hierarchical kernels once per call; the per-colour form once per colour
+    # and iteration
     st0 = plan.stats()
-    launches = {"atomic": args.steps, "hier": 1}.get(chosen.exec, args.steps * st0["n_colours"])
+    if chosen.exec == "atomic":
+        launches = args.steps
+    elif chosen.exec == "hier" and st0["kernel"].startswith("split"):
+        launches = args.steps + (1 if st0["shared_points"] else 0)
+    elif chosen.exec == "hier":
+        launches = 1
+    else:
+        launches = args.steps * st0["n_colours"]
 
     # ---- timed region: inputs resident in HBM -------------------------------
     # K steps = one Plan.run(K) call (K iterations of the loop), as the
@@ -365,6 +385,32 @@ def main(argv=None):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(md)
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        from cuda_fot_b200 import bench_configs as BC
+        model = None
+        try:
+            model = CM.load_default()
+        except Exception:
+            pass
+        jobs = [("res_calc_1000", lambda: BC.res_calc_1000(model, peak, stream)),
+                ("lulesh_96", lambda: BC.lulesh_96(peak)),
+                ("atomic_spread", lambda: {
+                    "mini_aero_128": BC.atomic_spread(md, T.Candidate("rcm", 0, "atomic", 256, aggregate=False,
+                                                                      layout="soa")),
+                    "res_calc_1000": BC.atomic_spread(mg.res_calc(1000, 1000, 1),
+                                                      T.Candidate("rcm", 0, "atomic", 256, aggregate=False,
+                                                                  layout="soa"))}),
+                ("plan_build", BC.plan_build),
+                ("cost_model", BC.cost_model),
+                ("batch_512", BC.batch_512)]
+        for key, fn in jobs:
+            t_job = time.perf_counter()
+            try:
+                extras[key] = fn()
+            except Exception as e:  # one configuration failing does not lose the others
+                extras[key] = {"error": f"{type(e).__name__}: {e}"}
+            extras[key]["wall_s"] = round(time.perf_counter() - t_job, 1)
 
     if rank == 0:
         st = plan.stats()
@@ -402,8 +448,17 @@ def main(argv=None):
             line["plan_judge"] = {"sweep_best": best["cand"].label(), "sweep_s": round(sweep_s, 1),
                                   "model_pick_s": round(pick_s, 1) if pick_s is not None else None,
                                   "regret": (mine["seconds"] / best["seconds"] - 1.0) if mine else None}
+        if sweep_res:
+            col = [r for r in sweep_res if r["ok"] and r["cand"].exec != "atomic"]
+            if col:
+                bc = min(col, key=lambda r: r["seconds"])
+                line["coloured"] = {"plan": bc["cand"].label(), "gbs": round(bc["gbs"], 1),
+                                    "frac": round(bc["gbs"] / peak, 4),
+                                    "speedup_vs_plain_atomics": round(atomic_plain["seconds"] / bc["seconds"], 3)
+                                    if atomic_plain.get("ok") else None}
         if choice_note:
             line["plan_note"] = choice_note
+        line.update(extras)
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -58,12 +58,9 @@ def timed(fn, stream, reps=1):
     return a.elapsed_time(b) / 1e3 / reps
 
 
-def main(argv=None) -> int:
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--meshes", type=int, default=512)
-    ap.add_argument("--timesteps", type=int, default=100)
-    ap.add_argument("--seed", type=int, default=1)
-    a = ap.parse_args(argv)
+def run(meshes: int = 512, timesteps: int = 100, seed: int = 1) -> dict:
+    """The batch benchmark; returns its JSON line as a dict."""
+    a = argparse.Namespace(meshes=meshes, timesteps=timesteps, seed=seed)
     import torch
     from . import fot as F
     from . import meshgen as mg
@@ -167,7 +164,16 @@ def main(argv=None) -> int:
             "speedup_batch_graph_vs_loop_atomic": res["loop_atomic"] / res["batch_graph"],
             "speedup_batch_graph_vs_loop_atomic_graph": res["loop_atomic_graph"] / res["batch_graph"],
             "host_s": {"mesh_generation": round(gen_s, 1), "upload": round(upload_s, 1)}}
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--meshes", type=int, default=512)
+    ap.add_argument("--timesteps", type=int, default=100)
+    ap.add_argument("--seed", type=int, default=1)
+    a = ap.parse_args(argv)
+    print(json.dumps(run(a.meshes, a.timesteps, a.seed)), flush=True)
     return 0
 
 

@@ -93,6 +93,11 @@ class OrderedCache:
         self.md = md
         self._cache: Dict = {}
 
+    def drop(self, order: Optional[str], partition: int) -> None:
+        """Forget the host copies of one ordering (both layouts)."""
+        for k in [k for k in self._cache if k[0] == order and k[1] == partition]:
+            del self._cache[k]
+
     def get(self, order: Optional[str], partition: int, layout: Optional[str] = None) -> mg.MeshData:
         if layout is not None and layout != self.md.layout:
             key = (order, partition, layout)
@@ -170,12 +175,20 @@ def measure(cache: OrderedCache, cand: Candidate, iters: int = 10, warmup: int =
 
 
 def sweep(md: mg.MeshData, cands: List[Candidate], iters: int = 10, warmup: int = 3,
-          verbose: bool = False) -> List[dict]:
-    cache = OrderedCache(md)
-    out = []
-    for c in cands:
-        r = measure(cache, c, iters, warmup)
-        out.append(r)
+          verbose: bool = False, cache: Optional[OrderedCache] = None) -> List[dict]:
+    """Measure every candidate, one (ordering, partition) at a time; the
+    host copies of an ordering are dropped once its candidates are measured
+    (the given cache keeps the unordered mesh only)."""
+    cache = cache or OrderedCache(md)
+    out = [None] * len(cands)
+    groups: Dict = {}
+    for i, c in enumerate(cands):
+        groups.setdefault((c.order, c.partition), []).append(i)
+    for key, idx in groups.items():
+        for i in idx:
+            out[i] = measure(cache, cands[i], iters, warmup)
+        cache.drop(*key)
+    for c, r in zip(cands, out):
         if verbose:
             if r["ok"]:
                 print(f"  {c.label():28s} {r['seconds']*1e6:9.1f} us  {r['gbs']:8.1f} GB/s", flush=True)
