@@ -102,7 +102,7 @@ def res_calc_1000(model, peak: float, stream) -> dict:
     for name, r in (("sweep_best", best), ("best_coloured", bc)):
         if r is None:
             continue
-        p, plan = T.build(cache.get(r["cand"].order, r["cand"].partition, r["cand"].layout), r["cand"])
+        p, plan = T.build(cache.get(r["cand"].order, r["cand"].partition), r["cand"])
         s = flushed_seconds(p, plan, 10, stream)
         flushed[name] = {"plan": r["cand"].label(), "us": round(s * 1e6, 2),
                          "gbs": round(ub / s / 1e9, 1), "frac": round(_frac(ub / s / 1e9, peak), 4)}

@@ -294,7 +294,7 @@ def generate(loops: Sequence[int], sizes: Sequence[float], seeds: Sequence[int],
                     orders_s += time.time() - t_o
                     for c in T.plan_candidates(order, part):
                         try:
-                            p, plan = T.build(cache.get(order, part, c.layout), c)
+                            p, plan = T.build(cache.get(order, part), c)
                             t1 = T.time_plan(p, plan, iters=2, warmup=1)
                             iters = int(min(50, max(3, iters_min_ms * 1e-3 / max(t1, 1e-7))))
                             secs = T.time_plan(p, plan, iters=iters, warmup=1)

@@ -378,6 +378,7 @@ int fot_plan_build(fot_problem *p, const fot_plan_desc *desc, fot_plan **out) {
   auto *plan = new fot_plan();
   plan->prob = p;
   plan->desc = *desc;
+  plan->point_layout = p->layout;
   const LoopOps *ops = loop_ops(p->loop);
   int rc = FOT_OK;
   if (desc->exec == FOT_EXEC_ATOMIC) {
@@ -543,6 +544,8 @@ static int run_plan(fot_problem *p, fot_plan *plan, uint32_t iterations, cudaStr
   const LoopData d = p->loop_data();
   const bool soa = p->layout == FOT_SOA;
   const int sms = device_sm_count();
+  if (plan->point_layout != p->layout)
+    return fail(FOT_ERR_STATE, "plan is stale: the problem's point layout changed after the plan was built");
   if (plan->desc.exec == FOT_EXEC_ATOMIC) {
     const bool agg = !(plan->desc.flags & FOT_PLAN_NO_AGGREGATE);
     const uint32_t need = (p->n_cells + 255) / 256;

@@ -112,6 +112,7 @@ struct fot_plan {
   fot_plan_desc desc{};
   fot_plan_stats stats{};
   uint32_t variant = 0; // hierarchical tile kernel variant (see LoopOps)
+  int point_layout = FOT_AOS; // the problem's point layout when the plan was built
   // hierarchical plans
   uint32_t n_blocks = 0, n_colours = 0;
   std::vector<uint32_t> colour_offsets; // host copy (n_colours + 1)

@@ -16,6 +16,8 @@
 //                          points (fot_plan_sector_count).
 // Counting uses (block, sector) keys, one radix sort and a distinct count,
 // all on the device; only the totals come back.
+//   fot_set_layout         point data AOS <-> SOA on the GPU (the reference
+//                          converts on the host, AOStoSOA, data_t.hpp:249-275)
 #include <algorithm>
 
 #include "devutil.cuh"
@@ -106,6 +108,52 @@ __global__ void k_count_distinct(const uint64_t *__restrict__ k, size_t n, unsig
   if ((threadIdx.x & 31u) == 0 && t) atomicAdd(count, (unsigned long long)t);
 }
 
+// Point-data layout conversion: tiles of kLayoutTile points staged in
+// shared memory so that both the AOS rows and the SOA component runs are
+// read and written coalesced.
+constexpr uint32_t kLayoutTile = 128;
+
+template <class T>
+__global__ void k_aos_to_soa(const T *__restrict__ src, T *__restrict__ dst, uint32_t n, uint32_t dim) {
+  extern __shared__ __align__(16) unsigned char tile_raw[];
+  T *tile = reinterpret_cast<T *>(tile_raw);
+  const uint32_t p0 = blockIdx.x * kLayoutTile;
+  const uint32_t np = min(kLayoutTile, n - p0);
+  for (uint32_t e = threadIdx.x; e < np * dim; e += blockDim.x) tile[e] = src[(size_t)p0 * dim + e];
+  __syncthreads();
+  for (uint32_t e = threadIdx.x; e < np * dim; e += blockDim.x) {
+    const uint32_t k = e / np, i = e - k * np;
+    dst[(size_t)k * n + p0 + i] = tile[i * dim + k];
+  }
+}
+
+template <class T>
+__global__ void k_soa_to_aos(const T *__restrict__ src, T *__restrict__ dst, uint32_t n, uint32_t dim) {
+  extern __shared__ __align__(16) unsigned char tile_raw[];
+  T *tile = reinterpret_cast<T *>(tile_raw);
+  const uint32_t p0 = blockIdx.x * kLayoutTile;
+  const uint32_t np = min(kLayoutTile, n - p0);
+  for (uint32_t e = threadIdx.x; e < np * dim; e += blockDim.x) {
+    const uint32_t k = e / np, i = e - k * np;
+    tile[i * dim + k] = src[(size_t)k * n + p0 + i];
+  }
+  __syncthreads();
+  for (uint32_t e = threadIdx.x; e < np * dim; e += blockDim.x) dst[(size_t)p0 * dim + e] = tile[e];
+}
+
+template <class T>
+int convert_layout(const void *src, void *dst, uint32_t n, uint32_t dim, bool to_soa) {
+  const size_t smem = (size_t)kLayoutTile * dim * sizeof(T);
+  const void *k = to_soa ? reinterpret_cast<const void *>(&k_aos_to_soa<T>)
+                         : reinterpret_cast<const void *>(&k_soa_to_aos<T>);
+  FOT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const T *s = static_cast<const T *>(src);
+  T *d = static_cast<T *>(dst);
+  void *args[] = {&s, &d, &n, &dim};
+  FOT_CUDA(cudaLaunchKernel(k, dim3((n + kLayoutTile - 1) / kLayoutTile), dim3(256), args, smem, 0));
+  return FOT_OK;
+}
+
 SectorRule sector_rule(const fot_problem *p, int layout) {
   SectorRule r;
   r.type_size = p->info.point_type_size[0];
@@ -164,6 +212,25 @@ int fot_mesh_features(fot_problem *p, double *out, int n_out) {
   out[0] = (double)mx;
   out[1] = (double)h[0] / n;
   for (int b = 0; b < 4; ++b) out[2 + b] = (double)h[2 + b] / np;
+  return FOT_OK;
+}
+
+int fot_set_layout(fot_problem *p, int layout) {
+  if (!p) return fail(FOT_ERR_ARG, "null problem");
+  if (layout != FOT_AOS && layout != FOT_SOA) return fail(FOT_ERR_ARG, "bad layout %d", layout);
+  if (layout == p->layout) return FOT_OK;
+  for (uint32_t k = 0; k < p->info.n_point_sets; ++k) {
+    const uint32_t dim = p->info.point_dim[k], ts = p->info.point_type_size[k];
+    if (dim == 1) continue;  // one component: both layouts are the same bytes
+    DevBuf nb;
+    FOT_TRY(nb.alloc(p->point_bytes(k)));
+    if (ts == 8) FOT_TRY(convert_layout<uint64_t>(p->point[k].ptr, nb.ptr, p->n_points[k], dim, layout == FOT_SOA));
+    else FOT_TRY(convert_layout<uint32_t>(p->point[k].ptr, nb.ptr, p->n_points[k], dim, layout == FOT_SOA));
+    FOT_CUDA(cudaDeviceSynchronize());
+    p->point[k] = std::move(nb);
+  }
+  p->layout = layout;
+  p->version++;  // plans built for the other layout are stale
   return FOT_OK;
 }
 

@@ -269,6 +269,12 @@ class Problem:
         _check(_lib.fot_get_cell_data(self._h, j, out.ctypes.data_as(C.c_void_p), C.c_size_t(out.nbytes)))
         return out
 
+    def set_layout(self, layout: str) -> None:
+        """Convert the point datasets to "aos" or "soa" on the GPU
+        (fot_set_layout; the reference's AOStoSOA runs on the host)."""
+        _check(_lib.fot_set_layout(self._h, SOA if layout == "soa" else AOS))
+        self.layout = layout
+
     read_point_data = set_point_data
     read_cell_data = set_cell_data
 

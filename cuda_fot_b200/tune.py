@@ -125,10 +125,10 @@ class OrderedCache:
 
 def build(md: mg.MeshData, cand: Candidate, stream=None):
     """A problem holding md (already ordered; converted to the candidate's
-    layout when it is not in it) and the candidate's plan."""
-    if md.layout != cand.layout:
-        md = md.to_layout(cand.layout)
+    point layout on the GPU when it is not in it) and the candidate's plan."""
     p = F.Problem.from_mesh(md)
+    if md.layout != cand.layout:
+        p.set_layout(cand.layout)
     flags = 0
     if cand.partition:
         p.set_partition(md.meta["partition_vector"])
@@ -159,7 +159,7 @@ def time_plan(p, plan, iters: int = 10, warmup: int = 3, stream=None) -> float:
 
 
 def measure(cache: OrderedCache, cand: Candidate, iters: int = 10, warmup: int = 3) -> dict:
-    md = cache.get(cand.order, cand.partition, cand.layout)
+    md = cache.get(cand.order, cand.partition)
     try:
         t0 = time.perf_counter()
         p, plan = build(md, cand)

@@ -140,6 +140,13 @@ int fot_set_point_data_async(fot_problem *p, uint32_t k, const void *host, size_
 int fot_get_point_data_async(fot_problem *p, uint32_t k, void *host, size_t bytes, void *stream);
 int fot_set_cell_data_async(fot_problem *p, uint32_t j, const void *host, size_t bytes, void *stream);
 
+/* Convert the problem's point datasets to `layout` (FOT_AOS or FOT_SOA) on the
+ * GPU, in place of the reference's host conversion AOStoSOA
+ * (data_t.hpp:249-275), both directions.  Plans built before become stale
+ * (fot_run then fails with FOT_ERR_STATE); device addresses of the point
+ * datasets change.  Synchronous. */
+int fot_set_layout(fot_problem *p, int layout);
+
 /* Device address of a dataset (owned by the problem; valid until the problem
  * is destroyed).  data_t::getDeviceData (data_t.hpp:48-52). */
 int fot_point_data_device(fot_problem *p, uint32_t k, void **dptr);

@@ -76,3 +76,35 @@ def test_mesh_features_match_numpy():
     want = [(deg <= 2).mean(), ((deg >= 3) & (deg <= 4)).mean(), ((deg >= 5) & (deg <= 6)).mean(),
             (deg >= 7).mean()]
     assert np.allclose(f["deg_hist"], want, rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("loop", range(5))
+def test_set_layout_matches_host_conversion_and_runs(loop):
+    """fot_set_layout converts every point dataset on the GPU, bit-identical
+    to the host conversion (the reference's AOStoSOA), both ways; plans built
+    before are stale; a plan on the converted problem gives the same result
+    as one on a problem created in SOA."""
+    from tests.helpers import bitwise_equal
+    md = {mg.RES_CALC: lambda: mg.res_calc(40, 30, 5), mg.MINI_AERO: lambda: mg.mini_aero(9, 5),
+          mg.LULESH: lambda: mg.lulesh(8, 5), mg.VOLNA: lambda: mg.volna(30, 20, 5),
+          mg.GETACC: lambda: mg.getacc(30, 20, 5)}[loop]()
+    soa = md.to_layout("soa")
+    p = F().Problem.from_mesh(md)
+    old = p.plan(F().EXEC_ATOMIC, 256)
+    p.set_layout("soa")
+    for k, d in enumerate(soa.point_data):
+        assert bitwise_equal(p.point_weights(k), d), k
+    with pytest.raises(F().FotError) as e:
+        old.run(1)
+    assert e.value.code == -3
+    plan = p.plan(F().EXEC_HIER, 64)
+    plan.run(2)
+    p.sync()
+    q = F().Problem.from_mesh(soa)
+    plan_q = q.plan(F().EXEC_HIER, 64)
+    plan_q.run(2)
+    q.sync()
+    assert bitwise_equal(p.point_weights(0), q.point_weights(0))
+    p.set_layout("aos")
+    for k in range(1, len(md.point_data)):
+        assert bitwise_equal(p.point_weights(k), md.point_data[k]), k
