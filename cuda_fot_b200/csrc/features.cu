@@ -154,6 +154,30 @@ int convert_layout(const void *src, void *dst, uint32_t n, uint32_t dim, bool to
   return FOT_OK;
 }
 
+__global__ void k_point_part_keys(const uint32_t *__restrict__ map, uint32_t n, int D,
+                                  const uint32_t *__restrict__ part, uint64_t *keys) {
+  const size_t ne = (size_t)n * D;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ne; e += (size_t)gridDim.x * blockDim.x)
+    keys[e] = ((uint64_t)map[e] << 32) | part[e / D];
+}
+
+// over distinct sorted (point, part) keys: points touched, and points
+// touched by at least two parts
+__global__ void k_point_sharing(const uint64_t *__restrict__ k, size_t n, unsigned long long *acc) {
+  unsigned int first = 0, second = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t q = (uint32_t)(k[i] >> 32);
+    const bool f = i == 0 || (uint32_t)(k[i - 1] >> 32) != q;
+    first += f;
+    second += !f && (i < 2 || (uint32_t)(k[i - 2] >> 32) != q);
+  }
+  const unsigned int a = __reduce_add_sync(0xFFFFFFFFu, first), b = __reduce_add_sync(0xFFFFFFFFu, second);
+  if ((threadIdx.x & 31u) == 0) {
+    atomicAdd(&acc[0], (unsigned long long)a);
+    atomicAdd(&acc[1], (unsigned long long)b);
+  }
+}
+
 SectorRule sector_rule(const fot_problem *p, int layout) {
   SectorRule r;
   r.type_size = p->info.point_type_size[0];
@@ -212,6 +236,49 @@ int fot_mesh_features(fot_problem *p, double *out, int n_out) {
   out[0] = (double)mx;
   out[1] = (double)h[0] / n;
   for (int b = 0; b < 4; ++b) out[2 + b] = (double)h[2 + b] / np;
+  return FOT_OK;
+}
+
+int fot_partition_quality(fot_problem *p, double *out, int n_out) {
+  if (!p || !out || n_out < FOT_PARTITION_QUALITY) return fail(FOT_ERR_ARG, "bad argument");
+  if (p->partition.size() != p->n_cells) return fail(FOT_ERR_STATE, "problem has no partition");
+  const uint32_t n = p->n_cells;
+  const int D = (int)p->mesh_dim();
+  std::vector<uint32_t> size;
+  for (uint32_t q : p->partition) {
+    if (q >= size.size()) size.resize(q + 1, 0);
+    ++size[q];
+  }
+  uint32_t parts = 0, largest = 0;
+  for (uint32_t sz : size)
+    if (sz) {
+      ++parts;
+      largest = std::max(largest, sz);
+    }
+  DevBuf part, keys, uniq, acc;
+  FOT_TRY(upload(part, p->partition));
+  const size_t ne = (size_t)n * D;
+  FOT_TRY(keys.alloc(2 * ne * 8));
+  FOT_TRY(uniq.alloc(ne * 8));
+  FOT_TRY(acc.alloc(16));
+  FOT_CUDA(cudaMemset(acc.ptr, 0, 16));
+  k_point_part_keys<<<std::min<uint32_t>(blocks_for(ne), 8192), 256>>>(p->map[0].as<uint32_t>(), n, D,
+                                                                        part.as<uint32_t>(),
+                                                                        keys.as<uint64_t>());
+  FOT_CUDA(cudaGetLastError());
+  uint64_t *k = keys.as<uint64_t>();
+  FOT_TRY(sort_keys(k, k + ne, ne));
+  uint32_t m = 0;
+  FOT_TRY(unique_keys(k + ne, uniq.as<uint64_t>(), ne, &m));
+  k_point_sharing<<<std::min<uint32_t>(blocks_for(m), 4096), 256>>>(uniq.as<uint64_t>(), m,
+                                                                     acc.as<unsigned long long>());
+  FOT_CUDA(cudaGetLastError());
+  unsigned long long h[2];
+  FOT_CUDA(cudaMemcpy(h, acc.ptr, 16, cudaMemcpyDeviceToHost));
+  out[0] = parts;
+  out[1] = parts ? largest / ((double)n / parts) : 0.0;
+  out[2] = h[0] ? (double)m / h[0] : 0.0;
+  out[3] = h[0] ? (double)h[1] / h[0] : 0.0;
   return FOT_OK;
 }
 

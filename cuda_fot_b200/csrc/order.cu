@@ -830,6 +830,169 @@ int grow_partition(fot_problem *p, uint32_t part_size, std::vector<uint32_t> &pa
   return download(part_out, part, n);
 }
 
+// ---------------------------------------------------------------------------
+// partitioning: recursive graph bisection over the cell-to-cell graph
+// ---------------------------------------------------------------------------
+// Every round, each segment that still holds k > 1 parts is cut in two: a
+// BFS restricted to the segment from its first cell finds a far cell (the
+// largest level, then the smallest id), a second restricted BFS from there
+// levels the segment along its longest extent, a stable sort by (segment,
+// level) orders its cells, and the first round(size * floor(k/2) / k) cells
+// form the part range [first, first + k/2), the rest [first + k/2, first +
+// k).  Parts end up within one cell of n / nparts, compact (each cut follows
+// a BFS front), and numbered so that neighbouring parts have nearby numbers.
+namespace {
+__global__ void k_seg_bfs_expand(const uint32_t *row, const uint32_t *col, const uint32_t *frontier,
+                                 uint32_t nf, const uint32_t *seg, uint32_t next_level, uint32_t *lvl,
+                                 uint32_t *next, uint32_t *n_next) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  const uint32_t u = frontier[i], su = seg[u];
+  for (uint32_t e = row[u]; e < row[u + 1]; ++e) {
+    const uint32_t v = col[e];
+    if (seg[v] == su && lvl[v] == INF && atomicCAS(&lvl[v], INF, next_level) == INF)
+      next[atomicAdd(n_next, 1u)] = v;
+  }
+}
+
+__global__ void k_gather_seeds(const uint32_t *perm, const uint32_t *pos, uint32_t m, uint32_t *seeds,
+                               uint32_t *lvl) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  const uint32_t c = pos ? perm[pos[j]] : perm[j];
+  seeds[j] = c;
+  lvl[c] = 0;
+}
+
+__global__ void k_seg_far(const uint32_t *lvl, const uint32_t *seg, uint32_t n, unsigned long long *best) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n || lvl[c] == INF) return;
+  atomicMax(&best[seg[c]], ((unsigned long long)lvl[c] << 32) | (INF - c));
+}
+
+__global__ void k_seg_keys(const uint32_t *perm, uint32_t n, const uint32_t *seg, const uint32_t *lvl,
+                           uint64_t *keys) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t c = perm[i];
+  keys[i] = ((uint64_t)seg[c] << 32) | lvl[c];
+}
+
+__global__ void k_seg_split(const uint32_t *perm, uint32_t n, uint32_t *seg, const uint32_t *start_of,
+                            const uint32_t *nleft_of, const uint32_t *k_of) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t c = perm[i], s = seg[c], k = k_of[s];
+  if (k > 1 && i - start_of[s] >= nleft_of[s]) seg[c] = s + k / 2;
+}
+
+// multi-source BFS restricted to segments; lvl[seeds] must be 0, the rest INF
+int seg_bfs(const Csr &g, const DevBuf &seg, DevBuf &lvl, DevBuf &fa, DevBuf &fb, DevBuf &cnt,
+            uint32_t n_seeds) {
+  uint32_t nf = n_seeds, level = 0;
+  while (nf) {
+    FOT_CUDA(cudaMemsetAsync(cnt.ptr, 0, 4));
+    k_seg_bfs_expand<<<blocks_for(nf), 256>>>(g.row.as<uint32_t>(), g.col.as<uint32_t>(),
+                                              fa.as<uint32_t>(), nf, seg.as<uint32_t>(), level + 1,
+                                              lvl.as<uint32_t>(), fb.as<uint32_t>(), cnt.as<uint32_t>());
+    FOT_CUDA(cudaMemcpy(&nf, cnt.ptr, 4, cudaMemcpyDeviceToHost));
+    std::swap(fa, fb);
+    ++level;
+  }
+  return FOT_OK;
+}
+} // namespace
+
+int bisect_partition(fot_problem *p, uint32_t part_size, std::vector<uint32_t> &part_out) {
+  const uint32_t n = p->n_cells;
+  const uint32_t nparts = (n + part_size - 1) / part_size;
+  Csr g;
+  FOT_TRY(cell_graph(p, g));
+  struct Seg {
+    uint32_t first, k, start, size;
+  };
+  std::vector<Seg> segs{{0, nparts, 0, n}};
+  std::vector<uint32_t> iota(n);
+  std::iota(iota.begin(), iota.end(), 0u);
+  DevBuf seg, perm, perm2, keys, keys2, lvl, fa, fb, cnt, best, d_start, d_nleft, d_k, d_pos;
+  FOT_TRY(seg.alloc((size_t)n * 4));
+  FOT_CUDA(cudaMemset(seg.ptr, 0, (size_t)n * 4));
+  FOT_TRY(upload(perm, iota));
+  FOT_TRY(perm2.alloc((size_t)n * 4));
+  FOT_TRY(keys.alloc((size_t)n * 8));
+  FOT_TRY(keys2.alloc((size_t)n * 8));
+  FOT_TRY(lvl.alloc((size_t)n * 4));
+  FOT_TRY(fa.alloc((size_t)n * 4));
+  FOT_TRY(fb.alloc((size_t)n * 4));
+  FOT_TRY(cnt.alloc(4));
+  FOT_TRY(best.alloc((size_t)nparts * 8));
+  for (int round = 0;; ++round) {
+    std::vector<uint32_t> act;  // indices into segs of segments still to cut
+    for (uint32_t i = 0; i < segs.size(); ++i)
+      if (segs[i].k > 1) act.push_back(i);
+    if (act.empty()) break;
+    if (round > 64) return fail(FOT_ERR_LIMIT, "partitioning did not converge");
+    const uint32_t m = (uint32_t)act.size();
+    std::vector<uint32_t> pos(m);
+    for (uint32_t j = 0; j < m; ++j) pos[j] = segs[act[j]].start;
+    FOT_TRY(upload(d_pos, pos));
+    // pass 1: from each segment's first cell, find a far cell
+    k_set_u32<<<blocks_for(n), 256>>>(lvl.as<uint32_t>(), n, INF);
+    k_gather_seeds<<<blocks_for(m), 256>>>(perm.as<uint32_t>(), d_pos.as<uint32_t>(), m,
+                                           fa.as<uint32_t>(), lvl.as<uint32_t>());
+    FOT_CUDA(cudaGetLastError());
+    FOT_TRY(seg_bfs(g, seg, lvl, fa, fb, cnt, m));
+    FOT_CUDA(cudaMemset(best.ptr, 0, (size_t)nparts * 8));
+    k_seg_far<<<blocks_for(n), 256>>>(lvl.as<uint32_t>(), seg.as<uint32_t>(), n,
+                                      best.as<unsigned long long>());
+    FOT_CUDA(cudaGetLastError());
+    std::vector<unsigned long long> h_best;
+    FOT_TRY(download(h_best, best.as<unsigned long long>(), nparts));
+    std::vector<uint32_t> far(m);
+    for (uint32_t j = 0; j < m; ++j) far[j] = INF - (uint32_t)(h_best[segs[act[j]].first] & 0xFFFFFFFFull);
+    // pass 2: level each segment from its far cell
+    DevBuf d_far;
+    FOT_TRY(upload(d_far, far));
+    k_set_u32<<<blocks_for(n), 256>>>(lvl.as<uint32_t>(), n, INF);
+    k_gather_seeds<<<blocks_for(m), 256>>>(d_far.as<uint32_t>(), nullptr, m, fa.as<uint32_t>(),
+                                           lvl.as<uint32_t>());
+    FOT_CUDA(cudaGetLastError());
+    FOT_TRY(seg_bfs(g, seg, lvl, fa, fb, cnt, m));
+    // order every segment by level (stable: ties keep the previous order)
+    k_seg_keys<<<blocks_for(n), 256>>>(perm.as<uint32_t>(), n, seg.as<uint32_t>(), lvl.as<uint32_t>(),
+                                       keys.as<uint64_t>());
+    FOT_CUDA(cudaGetLastError());
+    FOT_TRY(sort_pairs(keys.as<uint64_t>(), keys2.as<uint64_t>(), perm.as<uint32_t>(),
+                       perm2.as<uint32_t>(), n));
+    std::swap(perm, perm2);
+    // cut
+    std::vector<uint32_t> start_of(nparts, 0), nleft_of(nparts, 0), k_of(nparts, 1);
+    std::vector<Seg> next;
+    for (const Seg &sg : segs) {
+      start_of[sg.first] = sg.start;
+      k_of[sg.first] = sg.k;
+      nleft_of[sg.first] = sg.size;
+      if (sg.k == 1) {
+        next.push_back(sg);
+        continue;
+      }
+      const uint32_t kl = sg.k / 2;
+      const uint32_t nl = (uint32_t)(((uint64_t)2 * sg.size * kl + sg.k) / (2 * (uint64_t)sg.k));
+      nleft_of[sg.first] = nl;
+      next.push_back({sg.first, kl, sg.start, nl});
+      next.push_back({sg.first + kl, sg.k - kl, sg.start + nl, sg.size - nl});
+    }
+    FOT_TRY(upload(d_start, start_of));
+    FOT_TRY(upload(d_nleft, nleft_of));
+    FOT_TRY(upload(d_k, k_of));
+    k_seg_split<<<blocks_for(n), 256>>>(perm.as<uint32_t>(), n, seg.as<uint32_t>(), d_start.as<uint32_t>(),
+                                        d_nleft.as<uint32_t>(), d_k.as<uint32_t>());
+    FOT_CUDA(cudaGetLastError());
+    segs.swap(next);
+  }
+  return download(part_out, seg, n);
+}
+
 } // namespace fot
 
 using namespace fot;
@@ -884,15 +1047,40 @@ int fot_reorder(fot_problem *p, int order, uint64_t seed) {
   return FOT_OK;
 }
 
-int fot_partition(fot_problem *p, uint32_t part_size, uint64_t seed) {
-  (void)seed;
+int fot_partition_tol(fot_problem *p, uint32_t part_size, float tolerance, int method) {
   if (!p) return fail(FOT_ERR_ARG, "null problem");
   if (part_size == 0) return fail(FOT_ERR_ARG, "part size must be positive");
+  if (!(tolerance >= 1.0f)) return fail(FOT_ERR_ARG, "tolerance must be at least 1 (got %g)", tolerance);
   std::vector<uint32_t> part;
-  FOT_TRY(grow_partition(p, part_size, part));
+  if (method == FOT_PARTITION_BISECT) {
+    FOT_TRY(bisect_partition(p, part_size, part));
+  } else if (method == FOT_PARTITION_GROW) {
+    FOT_TRY(grow_partition(p, part_size, part));
+  } else {
+    return fail(FOT_ERR_ARG, "unknown partitioning method %d", method);
+  }
+  if (method == FOT_PARTITION_BISECT) {
+    // the load-balance bound of the reference's METIS call (ubvec =
+    // tolerance, partition.cu:18-29): parts of at most tolerance x the mean,
+    // up to the one cell that integral sizes need
+    std::vector<uint32_t> size;
+    for (uint32_t q : part) {
+      if (q >= size.size()) size.resize(q + 1, 0);
+      ++size[q];
+    }
+    const double mean = (double)p->n_cells / size.size();
+    for (uint32_t sz : size)
+      if (sz > tolerance * mean + 1.0)
+        return fail(FOT_ERR_STATE, "part of %u cells exceeds the tolerance bound %.1f", sz, tolerance * mean);
+  }
   p->partition.swap(part);
   FOT_CUDA(cudaDeviceSynchronize());
   return FOT_OK;
+}
+
+int fot_partition(fot_problem *p, uint32_t part_size, uint64_t seed) {
+  (void)seed;  // both methods are deterministic
+  return fot_partition_tol(p, part_size, 1.001f, FOT_PARTITION_BISECT);
 }
 
 int fot_reorder_to_partition(fot_problem *p) {

@@ -33,6 +33,7 @@ EXEC_ATOMIC, EXEC_HIER, EXEC_HIER_LAUNCH = 0, 1, 2
 ORDER_NATURAL, ORDER_RANDOM, ORDER_RCM, ORDER_GPS = 0, 1, 2, 3
 PLAN_NO_AGGREGATE, PLAN_USE_PARTITION, PLAN_DIRECT_READS, PLAN_SIMPLE_TILES = 1, 2, 4, 8
 PLAN_BLOCK_FLAGS = 16
+PARTITION_BISECT, PARTITION_GROW = 0, 1
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(f"{LIB_PATH} is missing: build it with `python -m cuda_fot_b200.build`")
@@ -336,8 +337,20 @@ class Problem:
     def reorder(self, order: int = ORDER_GPS, seed: int = 1) -> None:
         _check(_lib.fot_reorder(self._h, order, C.c_uint64(seed)))
 
-    def partition(self, part_size: int, seed: int = 1) -> None:
-        _check(_lib.fot_partition(self._h, part_size, C.c_uint64(seed)))
+    def partition(self, part_size: int, seed: int = 1, tolerance: float = 1.001,
+                  method: str = "bisect") -> None:
+        """fot_partition_tol: ceil(n_cells / part_size) parts by recursive
+        graph bisection ("bisect") or region growing ("grow")."""
+        m = {"bisect": PARTITION_BISECT, "grow": PARTITION_GROW}[method]
+        _check(_lib.fot_partition_tol(self._h, C.c_uint32(part_size), C.c_float(tolerance), C.c_int(m)))
+
+    def partition_quality(self) -> dict:
+        """fot_partition_quality: parts, balance, (part, point) pairs per point
+        and the fraction of points shared by parts."""
+        out = (C.c_double * 4)()
+        _check(_lib.fot_partition_quality(self._h, out, C.c_int(4)))
+        return {"parts": int(out[0]), "max_over_mean": out[1], "pairs_per_point": out[2],
+                "shared_points": out[3]}
 
     def reorder_to_partition(self) -> None:
         _check(_lib.fot_reorder_to_partition(self._h))

@@ -173,11 +173,32 @@ int fot_get_cell_order(fot_problem *p, uint32_t *host);
  * (mesh.hpp:199-225) and SCOTCH's GPS ordering (reorder.hpp:135-175). */
 int fot_reorder(fot_problem *p, int order, uint64_t seed);
 
-/* Partition the cells into parts of at most part_size cells by growing
- * connected parts over the cell-to-cell graph on the GPU.  The partition is
- * stored on the problem (Problem::partition_vector).  Replaces
- * Problem::partition / partitionOurs (problem.hpp:484-515) and METIS. */
+/* Partition the cells into ceil(n_cells / part_size) parts on the GPU; the
+ * partition is stored on the problem (Problem::partition_vector).  Replaces
+ * Problem::partition / partitionOurs (problem.hpp:484-515), METIS k-way
+ * (partition.cu:11-31) and the heuristic block growth (partition.cu:42-215).
+ * Methods:
+ *   FOT_PARTITION_BISECT  recursive graph bisection of the cell-to-cell graph
+ *                         (each cut along a BFS front of the segment from a
+ *                         far cell); parts within one cell of the mean size;
+ *   FOT_PARTITION_GROW    parts grown from seeds over the cell-to-cell graph,
+ *                         at most part_size cells each (more, smaller parts).
+ * tolerance (>= 1): the reference's load-balance bound (METIS ubvec): with
+ * BISECT no part exceeds tolerance x the mean size by more than one cell
+ * (checked; FOT_ERR_STATE otherwise). */
+#define FOT_PARTITION_BISECT 0
+#define FOT_PARTITION_GROW 1
+int fot_partition_tol(fot_problem *p, uint32_t part_size, float tolerance, int method);
+/* fot_partition_tol(p, part_size, 1.001, FOT_PARTITION_BISECT); seed unused
+ * (both methods are deterministic). */
 int fot_partition(fot_problem *p, uint32_t part_size, uint64_t seed);
+/* Quality of the problem's partition against mapping 0, on the GPU:
+ * out[0] parts, out[1] largest / mean part size, out[2] (part, point) pairs
+ * per point touched -- the points a hierarchical block stages and writes per
+ * point, 1 when no point is shared --, out[3] the fraction of points touched
+ * by more than one part. */
+#define FOT_PARTITION_QUALITY 4
+int fot_partition_quality(fot_problem *p, double *out, int n_out);
 /* Problem::reorderToPartition (problem.hpp:517-526): cells sorted by part. */
 int fot_reorder_to_partition(fot_problem *p);
 /* Problem::renumberPoints (problem.hpp:528-551): points renumbered by the

@@ -214,11 +214,18 @@ template <bool SOA = false> class Problem {
     check(fot_reorder(h_, order, 1));
     pull(true);
   }
-  void partition(float /*tolerance*/) {
+  // METIS k-way with load-balance tolerance (problem.hpp:484-499): recursive
+  // graph bisection on the GPU into ceil(numCells / block_size) parts, no
+  // part above tolerance x the mean (+1 cell)
+  void partition(float tolerance) {
     push();
-    check(fot_partition(h_, block_size, 1));
+    check(fot_partition_tol(h_, block_size, tolerance, FOT_PARTITION_BISECT));
     pull(true);
   }
+  // METIS coarse parts of block_size x num_blocks_in_coarse cells refined by
+  // the heuristic growth (problem.hpp:501-515): the bisection is already
+  // hierarchical -- its first rounds cut the coarse parts -- so the fine
+  // parts come from the same call
   void partitionOurs(float tolerance, MY_SIZE /*num_blocks_in_coarse*/) { partition(tolerance); }
   void reorderToPartition() {
     push();

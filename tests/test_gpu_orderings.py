@@ -113,8 +113,12 @@ def test_partition_reorder_renumber(loop):
     p.partition(64)
     part = p.partition_vector()
     counts = np.bincount(part)
-    assert counts.max() <= 64 and counts.sum() == md.n_cells
-    assert (counts > 0).sum() <= 2 * int(np.ceil(md.n_cells / 64)) + 8
+    # ceil(n / 64) parts within one cell of the mean: the reference's METIS
+    # balance (tolerance 1.001) up to integral sizes
+    nparts = int(np.ceil(md.n_cells / 64))
+    assert counts.size == nparts and counts.sum() == md.n_cells
+    mean = md.n_cells / nparts
+    assert counts.max() <= min(64, np.ceil(mean)) and counts.min() >= np.floor(mean)
     p.reorder_to_partition()
     part2 = p.partition_vector()
     assert np.all(np.diff(part2.astype(np.int64)) >= 0)
@@ -149,3 +153,48 @@ def test_partition_blocks_follow_parts():
     p.sync()
     rep, _ = O.replay_hier(mdp, ex, 2)
     assert bitwise_equal(p.point_weights(0), rep[0])
+
+
+def quality_numpy(map0, part):
+    """(part, point) pairs per point and the fraction of shared points, from
+    the mapping and a partition (restated on the CPU)."""
+    pairs = np.unique(np.stack([map0.astype(np.int64).ravel(),
+                                np.repeat(part.astype(np.int64), map0.shape[1])], 1), axis=0)
+    pts, cnt = np.unique(pairs[:, 0], return_counts=True)
+    return len(pairs) / len(pts), float((cnt > 1).mean())
+
+
+@pytest.mark.parametrize("loop", [mg.RES_CALC, mg.LULESH, mg.GETACC, mg.MINI_AERO])
+def test_partition_quality_beats_contiguous_blocks(loop):
+    """The bisection's parts share fewer points than blocks of consecutive
+    cells of the RCM order (what the plan would form without a partition)
+    and than the region-growing parts; fot_partition_quality agrees with the
+    CPU restatement."""
+    md = {mg.RES_CALC: lambda: mg.res_calc(80, 60, 3), mg.MINI_AERO: lambda: mg.mini_aero(14, 3),
+          mg.LULESH: lambda: mg.lulesh(14, 3), mg.GETACC: lambda: mg.getacc(70, 50, 3)}[loop]()
+    res = {}
+    for method in ("bisect", "grow"):
+        p = F().Problem.from_mesh(md)
+        p.reorder(F().ORDER_RCM)
+        p.partition(128, method=method)
+        q = p.partition_quality()
+        ppp, shared = quality_numpy(p.mapping(0), p.partition_vector())
+        assert abs(q["pairs_per_point"] - ppp) < 1e-12 and abs(q["shared_points"] - shared) < 1e-12
+        res[method] = q
+    p = F().Problem.from_mesh(md)
+    p.reorder(F().ORDER_RCM)
+    contiguous, _ = quality_numpy(p.mapping(0), np.arange(md.n_cells) // 128)
+    assert res["bisect"]["parts"] == int(np.ceil(md.n_cells / 128))
+    assert res["bisect"]["max_over_mean"] <= 1.0 + res["bisect"]["parts"] / md.n_cells + 1e-12
+    assert res["bisect"]["pairs_per_point"] < contiguous
+    assert res["bisect"]["pairs_per_point"] <= res["grow"]["pairs_per_point"]
+
+
+def test_partition_tolerance_is_checked():
+    p = F().Problem.from_mesh(mg.res_calc(20, 20, 1))
+    with pytest.raises(F().FotError) as e:
+        p.partition(32, tolerance=0.9)
+    assert e.value.code == -1
+    p.partition(32, tolerance=1.0)
+    counts = np.bincount(p.partition_vector())
+    assert counts.max() - counts.min() <= 1
