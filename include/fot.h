@@ -346,15 +346,18 @@ int fot_model_predict(fot_model *m, const float *X, int n, float *y);
  * reference).  For callers that must not allocate device memory once they
  * are running: the inputs and outputs of the call are staged in a fixed
  * file-scope device array of FOT_MODEL_NOALLOC_MAX_ROWS rows (25 floats per
- * row, 409,600 bytes, held on every GPU that loads the library until the
- * process exits) instead of buffers allocated per call.  More rows
- * than that: FOT_ERR_LIMIT, nothing is computed.  No part of the array has
- * to start at zero (a call writes every row it reads).  All calls on one
- * device share the array, so calls that overlap in time (from several host
- * threads) race and must be serialised by the caller.  The first call on a
- * device does the setup (looks up the array's address, sets the kernel's
- * shared-memory limit) and should come before any stream capture.  Same
- * results as fot_model_predict.  Synchronous. */
+ * row, 409,600 bytes) instead of buffers allocated per call.  The array
+ * exists on a device once the library's module is loaded there -- with
+ * CUDA's lazy module loading, from the first use on that device -- and stays
+ * until the process exits.  More rows than the maximum: FOT_ERR_LIMIT,
+ * nothing is computed.  No part of the array has to start at zero (a call
+ * writes every row it reads).  All calls on one device share the array, so
+ * calls that overlap in time (from several host threads) race and must be
+ * serialised by the caller.  The first call on a device does the setup
+ * (looks up the array's address, sets the kernel's shared-memory limit) and
+ * should come before any stream capture.  Same results as
+ * fot_model_predict.  Synchronous: inputs and outputs move with cudaMemcpy
+ * and the kernel runs on the legacy default stream. */
 #define FOT_MODEL_NOALLOC_MAX_ROWS 4096
 int fot_model_predict_noalloc(fot_model *m, const float *X, int n, float *y);
 /* gradient of 0.5/n * sum (model(X) - t)^2 w.r.t. the parameters, and the loss */
