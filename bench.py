@@ -377,6 +377,19 @@ def main(argv=None):
     e2e_secs = max_over_ranks(s2.elapsed_time(e2) / 1e3, world)
     e2e_value = ub * e2e_steps * world / e2e_secs / 1e9
 
+    # the reference's sector model for the plan that ran (blocks of 256
+    # consecutive cells for the atomic executor, as its global-colour loop
+    # counts them; the plan's blocks otherwise): sectors x 32 B x 2 per
+    # iteration is its "cache line" bandwidth (problem.hpp:189-192)
+    try:
+        if chosen.exec == "atomic":
+            sectors, _ = p.sector_count(256)
+        else:
+            sectors, _ = plan.sector_count()
+        sector_model = {"sectors_per_iteration": int(sectors), "bytes_per_iteration": int(sectors) * 64,
+                        "gbs": int(sectors) * 64 / (secs / args.steps) / 1e9}
+    except Exception as e:
+        sector_model = {"error": str(e)}
     peak, peak_src = load_peaks()
     # algorithmic bytes per iteration / device time per iteration of this rank
     achieved = ub / (secs / args.steps) / 1e9
@@ -438,6 +451,7 @@ def main(argv=None):
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
+            "sector_model": sector_model,
             "gpu_launches": launches,
             "clocks": clocks.summary(),
         }

@@ -30,7 +30,7 @@
 //     plan-ordered mapping (like the atomic executor: thousands of
 //     independent gathers in flight per SM), adds its increments into a
 //     shared-memory sum one thread colour after another, and the block's
-//     sums go out as above.  Extra CTAs at the front of the grid do the
+//     sums go out as above.  Extra CTAs at the end of the grid do the
 //     combine.
 //   * k_hier_split (staged): persistent CTAs of T compute threads and two
 //     control warps; the RECORD warp bulk-copies each tile's record (plan.cu,
@@ -132,8 +132,8 @@ __device__ __forceinline__ void split_writeback(const LoopData &d, const HierPla
   }
 }
 
-// Direct form: CTAs [0, comb_ctas) combine the previous buffer, the others
-// run one tile each (hardware CTA scheduling keeps several tiles per SM in
+// Direct form: CTAs [0, n_blocks) run one tile each, the comb_ctas after
+// them combine the previous buffer (hardware CTA scheduling keeps several tiles per SM in
 // different phases; a persistent form with one tile in flight per CTA and
 // the next tile's plan data prefetched measured slower).  A tile is the
 // reference's block step with HBM/L2 gathers: one thread per cell gathers its
@@ -152,16 +152,19 @@ __global__ void __launch_bounds__(T, hier_min_blocks<L, T>()) k_hier_dsplit(Loop
   out_t *const acc = reinterpret_cast<out_t *>(smem);
   const uint32_t tid = threadIdx.x;
   griddep_launch_dependents();
-  if (blockIdx.x < P.comb_ctas) {
+  const uint32_t n_tiles = P.tiles_on ? P.n_blocks : 0u;
+  if (blockIdx.x >= n_tiles) {
+    // the combine CTAs come last, so that the tiles are scheduled first
+    // (they gather and compute before their wait; these only wait)
     griddep_wait();
     if (P.comb_on) {
       uint32_t g0, g1;
-      comb_chunk(P.n_shared, blockIdx.x, P.comb_ctas, g0, g1);
+      comb_chunk(P.n_shared, blockIdx.x - n_tiles, P.comb_ctas, g0, g1);
       combine_shared<L, SOA>(d, P, g0, g1, tid, T);
     }
     return;
   }
-  const uint4 h = __ldg(P.tile_hdr + (blockIdx.x - P.comb_ctas));
+  const uint4 h = __ldg(P.tile_hdr + blockIdx.x);
   const uint32_t start = h.x, ncell = h.y & 0xFFFFu, ntcol = h.y >> 16, n0 = h.z, poff = h.w;
   for (uint32_t e = tid; e < n0 * K; e += T) acc[e] = out_t(0);
   // this thread's first written point (issued early; used after the sums)
