@@ -436,6 +436,16 @@ int fot_plan_build(fot_problem *p, const fot_plan_desc *desc, fot_plan **out) {
     if (rc == FOT_OK)
       rc = ops->occupancy(desc->exec, p->layout == FOT_SOA, plan->threads, plan->variant,
                           plan->smem, &plan->per_sm);
+    if (rc == FOT_OK && plan->per_sm == 0 && (plan->variant & kVariantPipe)) {
+      // the two-tile layout fits the limit but not beside the kernel's own
+      // shared memory: the single-buffer persistent kernel runs the plan
+      plan->variant &= ~(kVariantPipe | kVariantSplit);
+      ops->smem_layout(plan->cap[0], plan->cap[1], plan->variant, plan->rec_cap, plan->threads,
+                       &plan->layout);
+      plan->smem = plan->layout.total;
+      rc = ops->occupancy(desc->exec, p->layout == FOT_SOA, plan->threads, plan->variant,
+                          plan->smem, &plan->per_sm);
+    }
     if (rc == FOT_OK && plan->per_sm == 0)
       rc = fail(FOT_ERR_LIMIT, "hierarchical kernel cannot be resident (%zu B smem, %u threads)",
                 plan->smem, plan->threads);
