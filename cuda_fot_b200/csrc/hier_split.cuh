@@ -143,8 +143,12 @@ __device__ __forceinline__ void split_writeback(const LoopData &d, const HierPla
 // replay's order, bit for bit); then each written point's sum goes out (RED
 // for private points, the slot for shared ones).  The tile header (start,
 // cells | colours << 16, written points, their offset) is one 16-byte load.
+template <class L, int T> constexpr int dsplit_min_blocks() {
+  return (65536 / (T * L::kDirectRegCap)) > 0 ? 65536 / (T * L::kDirectRegCap) : 1;
+}
+
 template <class L, bool SOA, int T>
-__global__ void __launch_bounds__(T, hier_min_blocks<L, T>()) k_hier_dsplit(LoopData d, HierPlanDev P) {
+__global__ void __launch_bounds__(T, dsplit_min_blocks<L, T>()) k_hier_dsplit(LoopData d, HierPlanDev P) {
   using out_t = typename L::out_t;
   using read_t = typename L::read_t;
   constexpr int D = L::kDim, K = L::kOut;

@@ -95,6 +95,8 @@ struct Loop {
   static constexpr int kNumRead = 3;
   static constexpr bool kHasClass1 = true;
   static constexpr int kRegCap = 64; // registers per thread the tile kernels are held to
+  // registers per thread of the direct split write-back kernel
+  static constexpr int kDirectRegCap = 48;
   // resident 256-thread CTAs per SM the atomic executor is compiled for
   static constexpr int kAtomicMinBlocks = FOT_ATOMIC_MINB_RES_CALC;
   // read set r: x (set 1, class 1, dim 2), q (set 2, class 0, dim 4), adt (set 3, class 0, dim 1)
@@ -135,6 +137,8 @@ struct Loop {
   static constexpr int kNumRead = 1;
   static constexpr bool kHasClass1 = false;
   static constexpr int kRegCap = 128; // registers per thread the tile kernels are held to
+  // registers per thread of the direct split write-back kernel
+  static constexpr int kDirectRegCap = kRegCap;
   // resident 256-thread CTAs per SM the atomic executor is compiled for
   static constexpr int kAtomicMinBlocks = FOT_ATOMIC_MINB_MINI_AERO;
   __host__ __device__ static constexpr int read_set(int) { return 1; }
@@ -185,6 +189,8 @@ struct Loop {
   static constexpr int kNumRead = 1;
   static constexpr bool kHasClass1 = false;
   static constexpr int kRegCap = 96; // registers per thread the tile kernels are held to
+  // registers per thread of the direct split write-back kernel
+  static constexpr int kDirectRegCap = kRegCap;
   // resident 256-thread CTAs per SM the atomic executor is compiled for
   static constexpr int kAtomicMinBlocks = FOT_ATOMIC_MINB_LULESH;
   __host__ __device__ static constexpr int read_set(int) { return 1; }
@@ -233,6 +239,8 @@ struct Loop {
   static constexpr int kNumRead = 1;
   static constexpr bool kHasClass1 = false;
   static constexpr int kRegCap = 64; // registers per thread the tile kernels are held to
+  // registers per thread of the direct split write-back kernel
+  static constexpr int kDirectRegCap = kRegCap;
   // resident 256-thread CTAs per SM the atomic executor is compiled for
   static constexpr int kAtomicMinBlocks = FOT_ATOMIC_MINB_VOLNA;
   __host__ __device__ static constexpr int read_set(int) { return 1; }
@@ -275,6 +283,8 @@ struct Loop {
   static constexpr int kNumRead = 0;
   static constexpr bool kHasClass1 = false;
   static constexpr int kRegCap = 96; // registers per thread the tile kernels are held to
+  // registers per thread of the direct split write-back kernel
+  static constexpr int kDirectRegCap = kRegCap;
   // resident 256-thread CTAs per SM the atomic executor is compiled for
   static constexpr int kAtomicMinBlocks = FOT_ATOMIC_MINB_GETACC;
   __host__ __device__ static constexpr int read_set(int) { return 0; }
