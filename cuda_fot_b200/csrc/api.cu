@@ -619,8 +619,8 @@ int fot_sync(fot_problem *p, void *stream) {
 
 int fot_plan_inject_lost_flag(fot_plan *plan, uint32_t block) {
   if (!plan) return fail(FOT_ERR_ARG, "null plan");
-  if (!(plan->variant & kVariantPipe) || !plan->block_done.ptr)
-    return fail(FOT_ERR_STATE, "the plan does not run the pipelined hierarchical kernel");
+  if (!(plan->variant & kVariantPipe) || (plan->variant & kVariantSplit) || !plan->block_done.ptr)
+    return fail(FOT_ERR_STATE, "the plan does not run the block-flag hierarchical kernel");
   if (block >= plan->n_blocks) return fail(FOT_ERR_ARG, "block %u out of range (%u blocks)", block, plan->n_blocks);
   FOT_CUDA(cudaDeviceSynchronize());
   Ctl c{};

@@ -268,7 +268,8 @@ int fot_sync(fot_problem *p, void *stream);
 
 /* Fault injection for tests of the failure path (no counterpart in the
  * reference).  Zeroes the completion flag of `block` (plan order) of a
- * pipelined hierarchical plan that has run at least once, as if the block's
+ * block-flag hierarchical plan (FOT_PLAN_BLOCK_FLAGS; FOT_ERR_STATE for
+ * other plans, whose kernels read no flags) that has run at least once, as if the block's
  * last completion had been lost.  In the next fot_run the tiles that depend
  * on the block wait for it until their time limit (about 2 s), the kernel
  * returns early, and fot_sync reports FOT_ERR_DEVICE and resets the plan's

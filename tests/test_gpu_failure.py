@@ -88,3 +88,15 @@ def test_sync_reports_an_earlier_plans_failure_once():
         p.sync()
     assert e.value.code == -5
     p.sync()  # reported once; the plan was reset
+
+
+def test_flag_injection_needs_a_block_flag_plan():
+    """The split write-back kernels wait on no flag: injecting into such a
+    plan is refused."""
+    p = F().Problem.from_mesh(mg.res_calc(32, 24, 3))
+    plan = p.plan(F().EXEC_HIER, 64)
+    plan.run(1)
+    p.sync()
+    with pytest.raises(F().FotError) as e:
+        plan.inject_lost_flag(0)
+    assert e.value.code == -3
