@@ -1,7 +1,9 @@
 """The learned plan cost model.
 
-A 24 -> 64 -> 64 -> 1 MLP (libfot's fot_model_* kernels: forward, backward
-and Adam on the GPU) predicts log(seconds per iteration) of a candidate plan
+An ensemble of 24 -> 64 -> 64 -> 1 MLPs (libfot's fot_model_* kernels:
+forward, backward and Adam on the GPU; the members differ in their
+initialisation, their predictions are averaged) predicts log(seconds per
+iteration) of a candidate plan
 (ordering, partition, executor, block size, point layout;
 cuda_fot_b200.tune.Candidate),
 relative to the mean over the candidates timed on the same mesh, from
@@ -216,7 +218,50 @@ class CostModel:
         return m
 
 
-def load_default() -> Optional[CostModel]:
+class Ensemble:
+    """Several CostModels trained from different initialisations; the
+    prediction is the mean of their log-time predictions (the spread of a
+    single model's held-out regret over initialisations is larger than the
+    ensemble's)."""
+
+    def __init__(self, members: List[CostModel]):
+        self.members = list(members)
+
+    def predict(self, X: np.ndarray) -> np.ndarray:
+        return np.mean([m.predict(X) for m in self.members], axis=0)
+
+    def predict_noalloc(self, X: np.ndarray) -> np.ndarray:
+        return np.mean([m.predict_noalloc(X) for m in self.members], axis=0)
+
+    def fit(self, X: np.ndarray, t: np.ndarray, epochs: int, batch: int, lr: float) -> np.ndarray:
+        return np.array([m.fit(X, t, epochs=epochs, batch=batch, lr=lr, seed=i)
+                         for i, m in enumerate(self.members)])
+
+    def save(self, path: str) -> None:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        np.savez(path, params=np.stack([m.params() for m in self.members]),
+                 mean=np.stack([m.mean for m in self.members]),
+                 std=np.stack([m.std for m in self.members]), features=np.array(FEATURES))
+
+    @classmethod
+    def load(cls, path: str) -> "Ensemble":
+        z = np.load(path)
+        params, mean, std = z["params"], z["mean"], z["std"]
+        if params.ndim == 1:  # a single model
+            params, mean, std = params[None], mean[None], std[None]
+        members = []
+        for i in range(params.shape[0]):
+            m = CostModel()
+            m.set_params(params[i])
+            m.set_normalisation(mean[i], std[i])
+            members.append(m)
+        return cls(members)
+
+
+ENSEMBLE_MEMBERS = 4
+
+
+def load_default() -> Optional[Ensemble]:
     """The committed model, or None when there is none or it was trained on
     another feature list (then the measured sweep chooses)."""
     if not os.path.exists(DEFAULT_MODEL):
@@ -224,7 +269,7 @@ def load_default() -> Optional[CostModel]:
     z = np.load(DEFAULT_MODEL)
     if "features" not in z.files or [str(f) for f in z["features"]] != FEATURES:
         return None
-    return CostModel.load(DEFAULT_MODEL)
+    return Ensemble.load(DEFAULT_MODEL)
 
 
 # ---------------------------------------------------------------------------
@@ -356,7 +401,7 @@ def load_corpus(path: str = DEFAULT_CORPUS) -> dict:
 DEFAULT_PLAN = "gps/atomic/256"  # the method without the model: a fixed default
 
 
-def evaluate(model: CostModel, data: dict, mask: np.ndarray) -> dict:
+def evaluate(model, data: dict, mask: np.ndarray) -> dict:
     """Regret of the model's pick vs the measured best per mesh group, and the
     default plan's regret, over the rows selected by mask."""
     X = data["X"][mask]
@@ -380,7 +425,7 @@ def evaluate(model: CostModel, data: dict, mask: np.ndarray) -> dict:
             "picks": picks}
 
 
-def pick(model: CostModel, md: mg.MeshData, candidates: List[T.Candidate]) -> T.Candidate:
+def pick(model, md: mg.MeshData, candidates: List[T.Candidate]) -> T.Candidate:
     """The candidate with the smallest predicted time.  Each distinct
     ordering is applied to a problem holding only the mesh's mappings and its
     statistics are taken on the GPU (ordering_stats); nothing is timed."""
@@ -415,28 +460,30 @@ def centred_targets(y: np.ndarray, group: np.ndarray) -> np.ndarray:
 
 
 def train_and_evaluate(data: dict, holdout_seed: Optional[int] = None, epochs: int = 800,
-                       seed: int = 1, lr: float = 1e-3) -> tuple:
-    """Train on every seed but the held-out one (default: the largest) and
-    evaluate there: regret vs the sweep, the fixed default's regret, and the
-    tuning time the model saves on the held-out meshes."""
+                       seed: int = 1, lr: float = 1e-3, members: int = ENSEMBLE_MEMBERS) -> tuple:
+    """Train an ensemble of `members` models on every seed but the held-out
+    one (default: the largest) and evaluate there: regret vs the sweep, the
+    fixed default's regret, and the tuning time the model saves on the
+    held-out meshes."""
     info = json.loads(str(data["info"]))
     seed_of = {d["gid"]: d["seed"] for d in info}
     seeds = np.array([seed_of[int(g)] for g in data["group"]])
     hold = int(seeds.max()) if holdout_seed is None else int(holdout_seed)
     train = seeds != hold
-    m = CostModel(seed=seed)
+    m = Ensemble([CostModel(seed=seed + i) for i in range(members)])
     t0 = time.time()
     t = centred_targets(data["y"], data["group"])
-    # 800 epochs at 1e-3: the held-out regret's spread over initialisations
-    # is smaller than with 200 at 2e-3 (max regret 6% vs up to 17%)
-    losses = m.fit(data["X"][train], t[train], epochs=epochs, batch=256, lr=lr)
+    # 800 epochs at 1e-3 per member: the held-out regret's spread over
+    # initialisations is smaller than with 200 at 2e-3, and the ensemble's
+    # smaller than one member's
+    losses = m.fit(data["X"][train], t[train], epochs=epochs, batch=256, lr=lr)[:, -1]
     train_s = time.time() - t0
     ev = evaluate(m, data, ~train)
     held = [d for d in info if d["seed"] == hold]
     sweep_s = sum(d.get("sweep_s", 0.0) for d in held)
     orders_s = sum(d.get("pick_s", d.get("orders_s", 0.0)) for d in held)
     ev.update({"holdout_seed": hold, "train_rows": int(train.sum()), "test_rows": int((~train).sum()),
-               "final_loss": float(losses[-1]), "train_s": round(train_s, 2),
+               "members": members, "final_loss": float(np.mean(losses)), "train_s": round(train_s, 2),
                "heldout_sweep_s": round(sweep_s, 1), "heldout_model_inputs_s": round(orders_s, 1),
                "tuning_time_saved_frac": (1.0 - orders_s / sweep_s) if sweep_s > 0 else None})
     return m, ev

@@ -97,13 +97,15 @@ def test_gpu_training_fits_a_smooth_function():
 
 @pytest.mark.gpu
 def test_trained_model_regret_on_held_out_seeds():
-    """Train on the committed corpus's training seeds; on held-out seeds the
-    model's pick is within 5% of the measured best on average and beats the
-    fixed default plan (the method without the model)."""
+    """Train the ensemble on the committed corpus's training seeds; on
+    held-out seeds the model's pick is within 5% of the measured best on
+    average and within 10% on every mesh, and beats the fixed default plan
+    (the method without the model)."""
     from cuda_fot_b200 import costmodel as CM
     if not os.path.exists(CM.DEFAULT_CORPUS):
         pytest.skip("no committed corpus")
     data = CM.load_corpus()
     _, ev = CM.train_and_evaluate(data)
     assert ev["mean_regret"] <= 0.05, ev
+    assert ev["max_regret"] <= 0.10, ev
     assert ev["default_mean_regret"] is None or ev["mean_regret"] < ev["default_mean_regret"], ev
