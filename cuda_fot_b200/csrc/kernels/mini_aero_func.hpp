@@ -51,8 +51,9 @@ USER_FUNCTION_SIGNATURE(double flux[5], const double *RESTRICT cell_values_left,
     Pl[k] += tl * cell_limiters_left[k * cell_stride];
     Pr[k] += tr * cell_limiters_right[k * cell_stride];
   }
-  ma_inviscid_flux(Pl, Pr, flux, face_normal, face_tangent, face_binormal,
-                   face_stride);
+  // The viscous flux is evaluated before the inviscid one (the two are
+  // independent, so every value is the same): the gradients then die before
+  // the Roe flux's eigenvector matrices are live.
   double pf[5], gf[5][3];
 #pragma unroll
   for (int k = 0; k < 5; ++k) {
@@ -64,6 +65,8 @@ USER_FUNCTION_SIGNATURE(double flux[5], const double *RESTRICT cell_values_left,
   }
   double vf[5];
   ma_viscous_flux(gf, pf, face_normal, vf, face_stride);
+  ma_inviscid_flux(Pl, Pr, flux, face_normal, face_tangent, face_binormal,
+                   face_stride);
 #pragma unroll
   for (int k = 0; k < 5; ++k) flux[k] -= vf[k];
 }
