@@ -28,9 +28,9 @@
 //     hier_pipe.cuh).  The split write-back kernel (k_hier_split,
 //     hier_split.cuh, the default) makes no tile wait: points written by one
 //     block are added at once, points shared by several blocks through
-//     per-block partial sums that the last block to arrive adds in colour
-//     order.  The result is therefore deterministic and equal to replaying
-//     the colours in order on the CPU.
+//     per-block partial sums that the next launch (or a final combine-only
+//     launch) adds in colour order.  The result is therefore deterministic
+//     and equal to replaying the colours in order on the CPU.
 #pragma once
 
 #include <cstdint>

@@ -84,8 +84,8 @@ extern "C" {
                                      they conflict with, all iterations in one launch (the
                                      default is the split write-back kernel: no tile waits,
                                      points shared by several blocks are summed in colour
-                                     order by the last block to arrive, one launch per
-                                     iteration) */
+                                     order by the next launch, one launch per iteration
+                                     and a combine-only launch at the end of a call) */
 
 typedef struct fot_problem fot_problem;
 typedef struct fot_plan fot_plan;
