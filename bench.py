@@ -21,8 +21,9 @@ ranks processed / the max over ranks of the timed region.
 At N=1 the line also carries the other configurations under their own keys
 (cuda_fot_b200/bench_configs.py): res_calc 1000^2 with an L2-flushed timing,
 LULESH 96^3 before and after reordering, the 512-mesh batch, the cost
-model's held-out regret, the atomic executor's run-to-run spread and the
-plan-build times; --no-extras skips them.
+model's held-out regret, the atomic executor's run-to-run spread, the
+plan-build times and the Airfoil iteration around res_calc; --no-extras
+skips them.
 """
 from __future__ import annotations
 
@@ -245,7 +246,8 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the other configurations (res_calc 1000^2, LULESH 96^3, the 512-mesh "
-                         "batch, the cost model's held-out regret, the atomic spread, plan builds)")
+                         "batch, the cost model's held-out regret, the atomic spread, plan builds, "
+                         "the Airfoil iteration)")
     ap.add_argument("--plan", default=None,
                     help="force a plan by its label, order[+partN]/exec[d][-plain]/block[@soa], "
                          "e.g. rcm/atomic-plain/256@soa")
@@ -421,6 +423,7 @@ def main(argv=None):
                                                       T.Candidate("rcm", 0, "atomic", 256, aggregate=False,
                                                                   layout="soa"))}),
                 ("plan_build", BC.plan_build),
+                ("airfoil_1000", lambda: BC.airfoil_1000(peak, stream)),
                 ("cost_model", BC.cost_model),
                 ("batch_512", BC.batch_512)]
         for key, fn in jobs:

@@ -21,7 +21,12 @@ Each function returns a dict for one key of bench.py's JSON line:
   coloured executors are bit-reproducible);
 * ``plan_build``     GPU ordering and plan-build wall time for res_calc 1000^2
   and mini_aero 128^3, beside the reference's host builder
-  (HierarchicalColourMemory, colouring.hpp:44-147) timed on the same mesh.
+  (HierarchicalColourMemory, colouring.hpp:44-147) timed on the same mesh;
+* ``airfoil_1000``   the Airfoil solver iteration around res_calc (save_soln,
+  then twice adt_calc, res_calc, bres_calc, update: fot_airfoil_run) on the
+  1000 x 1000 mesh, with res_calc through the best atomic plan and through a
+  coloured one: time per iteration, GB/s of the iteration's unique bytes, and
+  the share of res_calc in it.
 """
 from __future__ import annotations
 
@@ -177,6 +182,65 @@ def atomic_spread(md: mg.MeshData, cand: T.Candidate, runs: int = 6) -> dict:
     diffs = [float(np.abs(o - ref).max() / den) for o in outs[1:]]
     return {"plan": cand.label(), "runs": runs, "max_normwise_diff": max(diffs),
             "identical_runs": int(sum(d == 0.0 for d in diffs)) + 1}
+
+
+def airfoil_unique_bytes(md: mg.MeshData, ex: dict) -> int:
+    """Algorithmic bytes of one Airfoil iteration: save_soln (q read, qold
+    written), and twice adt_calc (cell->node map, node coordinates, q, adt
+    written), res_calc (its unique bytes), bres_calc (boundary maps and
+    flags, the boundary cells' q, adt, res read and written) and update
+    (qold, q written, res read and written, adt)."""
+    nc, nn = md.n_points[0], md.n_points[1]
+    nb = len(ex["bedge_to_cell"])
+    nbc = len(np.unique(ex["bedge_to_cell"]))
+    save = nc * 64
+    adt = nc * 16 + nn * 16 + nc * 32 + nc * 8
+    bres = nb * (8 + 4 + 4) + nbc * (32 + 8 + 64)
+    update = nc * (32 + 32 + 64 + 8)
+    return save + 2 * (adt + md.unique_bytes() + bres + update)
+
+
+def airfoil_1000(peak: float, stream, iters: int = 20) -> dict:
+    import torch
+    md = mg.res_calc(1000, 1000, 1)
+    ex = mg.airfoil_extras(md)
+    ub = airfoil_unique_bytes(md, ex)
+    out = {"workload": "Airfoil iteration: save_soln + 2 x (adt_calc, res_calc, bres_calc, update) "
+                       "on res_calc 1000x1000 (1,998,000 edges, 4,000 boundary edges), FP64",
+           "unique_bytes_per_iteration": ub}
+    for name, (order, part, layout, exec_, block, flags) in (
+            ("atomic", ("rcm", 0, "soa", F.EXEC_ATOMIC, 256, F.PLAN_NO_AGGREGATE)),
+            ("coloured", ("rcm", 256, "aos", F.EXEC_HIER, 256, F.PLAN_USE_PARTITION))):
+        p = F.Problem.from_mesh(md)
+        p.reorder(T.ORDERS[order], seed=1)
+        if part:
+            p.partition(part)
+            p.reorder_to_partition()
+            p.renumber_points()
+        if layout != md.layout:
+            p.set_layout(layout)
+        plan = p.plan(exec_, block, flags)
+        af = F.Airfoil(p, ex["cell_to_node"], ex["bedge_to_node"], ex["bedge_to_cell"],
+                       ex["bound"], ex["qinf"], ex["cfl"])
+        af.run(plan, 3, stream, rms=False)
+        p.sync(stream)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        af.run(plan, iters, stream, rms=False)
+        b.record(stream)
+        b.synchronize()
+        secs = a.elapsed_time(b) / 1e3 / iters
+        rms = af.run(plan, 1, stream)
+        loop_s = T.time_plan(p, plan, iters, 3, stream)
+        label = f"{order}{'+part%d' % part if part else ''}/" + \
+                ("atomic-plain/256" if exec_ == F.EXEC_ATOMIC else f"hier/{block}") + \
+                ("@soa" if layout == "soa" else "")
+        out[name] = {"res_calc_plan": label, "us_per_iteration": round(secs * 1e6, 2),
+                     "gbs": round(ub / secs / 1e9, 1), "frac": round(_frac(ub / secs / 1e9, peak), 4),
+                     "res_calc_share": round(2 * loop_s / secs, 3), "rms_after": rms}
+        del af, plan, p
+    return out
 
 
 def plan_build() -> dict:

@@ -128,7 +128,12 @@ fot::LoopData fot_problem::loop_data() const {
     d.n_points[k] = n_points[k];
   }
   d.out = point[0].ptr;
-  for (uint32_t j = 0; j < info.n_cell_sets; ++j) d.cell[j] = cell[j].ptr;
+  for (uint32_t j = 0; j < info.n_cell_sets; ++j) {
+    d.cell[j] = cell[j].ptr;
+    d.cell_dim[j] = info.cell_dim[j];
+    d.cell_size[j] = info.cell_type_size[j];
+  }
+  d.n_cell_sets = info.n_cell_sets;
   d.n_cells = n_cells;
   return d;
 }
@@ -168,6 +173,8 @@ fot::HierPlanDev fot_plan::dev(uint32_t iterations) const {
   P.n_shared = n_shared_points;
   P.tiles_on = 1;
   P.ctl = ctl.as<Ctl>();
+  // the direct split kernel's CTAs resident at once (its prefetch distance)
+  if ((variant & kVariantSplit) && !(variant & kVariantPipe)) P.ahead = (uint32_t)(per_sm * device_sm_count());
   return P;
 }
 
@@ -255,8 +262,10 @@ int fot_problem_create(int loop, int layout, uint32_t n_cells, const uint32_t *n
 
 int fot_problem_destroy(fot_problem *p) {
   // plans outliving their problem fail with FOT_ERR_STATE from now on
-  if (p)
+  if (p) {
     for (fot_plan *plan : p->plans) plan->prob = nullptr;
+    for (fot_airfoil *a : p->airfoils) fot_airfoil_detach(a);
+  }
   delete p;
   return FOT_OK;
 }

@@ -94,6 +94,8 @@ struct fot_problem {
   std::vector<struct fot_plan *> pending;
   // live plans built on this problem (told when the problem is destroyed)
   std::vector<struct fot_plan *> plans;
+  // live Airfoil steps on this problem (told when the problem is destroyed)
+  std::vector<struct fot_airfoil *> airfoils;
 
   size_t point_bytes(uint32_t k) const {
     return (size_t)n_points[k] * info.point_dim[k] * info.point_type_size[k];
@@ -105,6 +107,9 @@ struct fot_problem {
   uint32_t mesh_dim() const { return info.mesh_dim[0]; }
   fot::LoopData loop_data() const;
 };
+
+// An Airfoil step whose problem is being destroyed (fails from now on).
+void fot_airfoil_detach(struct fot_airfoil *a);
 
 struct fot_plan {
   fot_problem *prob = nullptr;

@@ -70,6 +70,24 @@
 #ifndef FOT_ATOMIC_MINB_GETACC
 #define FOT_ATOMIC_MINB_GETACC 2
 #endif
+// Whether the atomic executor prefetches the next chunk's mapping rows and
+// direct data into L2 while it computes the current one (per loop; measured
+// choices, overridable at build time).
+#ifndef FOT_ATOMIC_PREFETCH_RES_CALC
+#define FOT_ATOMIC_PREFETCH_RES_CALC 0
+#endif
+#ifndef FOT_ATOMIC_PREFETCH_MINI_AERO
+#define FOT_ATOMIC_PREFETCH_MINI_AERO 1
+#endif
+#ifndef FOT_ATOMIC_PREFETCH_LULESH
+#define FOT_ATOMIC_PREFETCH_LULESH 0
+#endif
+#ifndef FOT_ATOMIC_PREFETCH_VOLNA
+#define FOT_ATOMIC_PREFETCH_VOLNA 0
+#endif
+#ifndef FOT_ATOMIC_PREFETCH_GETACC
+#define FOT_ATOMIC_PREFETCH_GETACC 0
+#endif
 #define FOT_STR2(x) #x
 #define FOT_STR(x) FOT_STR2(x)
 #define FOT_FUNCTOR(file) FOT_STR(FOT_FUNCTOR_DIR/file)
@@ -99,6 +117,8 @@ struct Loop {
   static constexpr int kDirectRegCap = 48;
   // resident 256-thread CTAs per SM the atomic executor is compiled for
   static constexpr int kAtomicMinBlocks = FOT_ATOMIC_MINB_RES_CALC;
+  // the atomic executor prefetches the next chunk into L2
+  static constexpr bool kAtomicPrefetch = FOT_ATOMIC_PREFETCH_RES_CALC;
   // read set r: x (set 1, class 1, dim 2), q (set 2, class 0, dim 4), adt (set 3, class 0, dim 1)
   __host__ __device__ static constexpr int read_set(int r) { return r + 1; }
   __host__ __device__ static constexpr int read_class(int r) { return r == 0 ? 1 : 0; }
@@ -141,6 +161,8 @@ struct Loop {
   static constexpr int kDirectRegCap = kRegCap;
   // resident 256-thread CTAs per SM the atomic executor is compiled for
   static constexpr int kAtomicMinBlocks = FOT_ATOMIC_MINB_MINI_AERO;
+  // the atomic executor prefetches the next chunk into L2
+  static constexpr bool kAtomicPrefetch = FOT_ATOMIC_PREFETCH_MINI_AERO;
   __host__ __device__ static constexpr int read_set(int) { return 1; }
   __host__ __device__ static constexpr int read_class(int) { return 0; }
   __host__ __device__ static constexpr int read_dim(int) { return 28; }
@@ -193,6 +215,8 @@ struct Loop {
   static constexpr int kDirectRegCap = kRegCap;
   // resident 256-thread CTAs per SM the atomic executor is compiled for
   static constexpr int kAtomicMinBlocks = FOT_ATOMIC_MINB_LULESH;
+  // the atomic executor prefetches the next chunk into L2
+  static constexpr bool kAtomicPrefetch = FOT_ATOMIC_PREFETCH_LULESH;
   __host__ __device__ static constexpr int read_set(int) { return 1; }
   __host__ __device__ static constexpr int read_class(int) { return 0; }
   __host__ __device__ static constexpr int read_dim(int) { return 3; }
@@ -243,6 +267,8 @@ struct Loop {
   static constexpr int kDirectRegCap = kRegCap;
   // resident 256-thread CTAs per SM the atomic executor is compiled for
   static constexpr int kAtomicMinBlocks = FOT_ATOMIC_MINB_VOLNA;
+  // the atomic executor prefetches the next chunk into L2
+  static constexpr bool kAtomicPrefetch = FOT_ATOMIC_PREFETCH_VOLNA;
   __host__ __device__ static constexpr int read_set(int) { return 1; }
   __host__ __device__ static constexpr int read_class(int) { return 0; }
   __host__ __device__ static constexpr int read_dim(int) { return 1; }
@@ -287,6 +313,8 @@ struct Loop {
   static constexpr int kDirectRegCap = kRegCap;
   // resident 256-thread CTAs per SM the atomic executor is compiled for
   static constexpr int kAtomicMinBlocks = FOT_ATOMIC_MINB_GETACC;
+  // the atomic executor prefetches the next chunk into L2
+  static constexpr bool kAtomicPrefetch = FOT_ATOMIC_PREFETCH_GETACC;
   __host__ __device__ static constexpr int read_set(int) { return 0; }
   __host__ __device__ static constexpr int read_class(int) { return 0; }
   __host__ __device__ static constexpr int read_dim(int) { return 1; }

@@ -215,6 +215,45 @@ class Batch:
             self._h = None
 
 
+class AirfoilDesc(C.Structure):
+    _fields_ = [("cell_to_node", u32p), ("n_bedges", C.c_uint32), ("bedge_to_node", u32p),
+                ("bedge_to_cell", u32p), ("bound", C.POINTER(C.c_int32)),
+                ("qinf", C.c_double * 4), ("cfl", C.c_double)]
+
+
+class Airfoil:
+    """The Airfoil solver iteration around a res_calc problem (fot_airfoil):
+    save_soln, then twice adt_calc, res_calc (through a plan), bres_calc and
+    update.  Maps are given in the problem's original numbering."""
+
+    def __init__(self, problem: "Problem", cell_to_node: np.ndarray, bedge_to_node: np.ndarray,
+                 bedge_to_cell: np.ndarray, bound: np.ndarray, qinf, cfl: float = 0.9):
+        self.problem = problem
+        self._keep = [np.ascontiguousarray(cell_to_node, dtype=np.uint32),
+                      np.ascontiguousarray(bedge_to_node, dtype=np.uint32),
+                      np.ascontiguousarray(bedge_to_cell, dtype=np.uint32),
+                      np.ascontiguousarray(bound, dtype=np.int32)]
+        c2n, b2n, b2c, bnd = self._keep
+        desc = AirfoilDesc(c2n.ctypes.data_as(u32p), C.c_uint32(len(b2c)), b2n.ctypes.data_as(u32p),
+                           b2c.ctypes.data_as(u32p), bnd.ctypes.data_as(C.POINTER(C.c_int32)),
+                           (C.c_double * 4)(*[float(v) for v in qinf]), C.c_double(cfl))
+        self._h = C.c_void_p()
+        _check(_lib.fot_airfoil_create(problem._h, C.byref(desc), C.byref(self._h)))
+
+    def run(self, plan: Plan, iterations: int = 1, stream=None, rms: bool = True):
+        """Runs `iterations` solver iterations with `plan` for res_calc;
+        returns the last iteration's rms (synchronising) or None."""
+        out = C.c_double()
+        _check(_lib.fot_airfoil_run(self._h, plan._h, C.c_uint32(iterations),
+                                    C.byref(out) if rms else None, _stream_ptr(stream)))
+        return out.value if rms else None
+
+    def __del__(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.fot_airfoil_destroy(self._h)
+            self._h = None
+
+
 class Problem:
     """A loop's mesh and datasets on the GPU (the reference's Problem<SOA>)."""
 

@@ -165,6 +165,35 @@ def res_calc(nx: int = 1000, ny: int = 1000, seed: int = 1,
     return md.to_layout(layout)
 
 
+def airfoil_extras(md: MeshData) -> dict:
+    """The data an Airfoil solver iteration needs beyond res_calc's, for a
+    mesh made by res_calc(nx, ny): each cell's 4 nodes counter-clockwise, the
+    4 (nx + ny) boundary edges (bottom, right, top, left) oriented like the
+    interior edges (with dx = x1 - x2, dy = y1 - y2 the normal (dy, -dx)
+    points out of the cell), solid walls at the bottom and top (bound 1),
+    far field left and right (bound 0), and the free stream
+    qinf = (1, 0.5, 0, 2.5) the generator's q perturbs."""
+    nx, ny = md.meta["nx"], md.meta["ny"]
+    node = lambda i, j: j * (nx + 1) + i  # noqa: E731
+    ii, jj = np.meshgrid(np.arange(nx), np.arange(ny))
+    ii, jj = ii.ravel(), jj.ravel()
+    c2n = np.stack([node(ii, jj), node(ii + 1, jj), node(ii + 1, jj + 1), node(ii, jj + 1)],
+                   axis=1).astype(np.uint32)
+    i = np.arange(nx)
+    j = np.arange(ny)
+    cell = lambda i, j: j * nx + i  # noqa: E731
+    bottom = (np.stack([node(i + 1, 0), node(i, 0)], 1), cell(i, 0), np.ones(nx))
+    right = (np.stack([node(nx, j + 1), node(nx, j)], 1), cell(nx - 1, j), np.zeros(ny))
+    top = (np.stack([node(i, ny), node(i + 1, ny)], 1), cell(i, ny - 1), np.ones(nx))
+    left = (np.stack([node(0, j), node(0, j + 1)], 1), cell(0, j), np.zeros(ny))
+    parts = (bottom, right, top, left)
+    return {"cell_to_node": c2n,
+            "bedge_to_node": np.concatenate([p[0] for p in parts]).astype(np.uint32),
+            "bedge_to_cell": np.concatenate([p[1] for p in parts]).astype(np.uint32),
+            "bound": np.concatenate([p[2] for p in parts]).astype(np.int32),
+            "qinf": np.array([1.0, 0.5, 0.0, 2.5]), "cfl": 0.9}
+
+
 # --------------------------------------------------------------------------
 # mini_aero: 3D face flux on a structured hex mesh
 # --------------------------------------------------------------------------

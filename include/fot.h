@@ -283,6 +283,43 @@ int fot_graph_create(fot_problem *p, fot_plan *plan, uint32_t iterations,
 int fot_graph_launch(fot_graph *g, void *stream);
 int fot_graph_destroy(fot_graph *g);
 
+/* ---- the Airfoil time step around res_calc ------------------------------ */
+
+/* The reference drives res_calc alone (res_calc.cu: Problem::loop*(num)).  An
+ * Airfoil solver iteration runs, on a res_calc problem's data (res = point set
+ * 0, x = 1 (nodes), q = 2, adt = 3, current numbering and layout):
+ *   save_soln  qold = q
+ *   2 x { adt_calc   per cell: adt = sum over its four sides (node j to j+1)
+ *                    of |u dy - v dx| + c |side|, divided by cfl
+ *                    (u, v = velocity, c = sound speed, gamma 1.4);
+ *         res_calc   one iteration of `plan` (atomic or hierarchical);
+ *         bres_calc  per boundary edge, in edge order per cell: a wall adds
+ *                    the pressure flux (res[1] += p dy, res[2] -= p dx), a
+ *                    far-field edge the res_calc flux against qinf with
+ *                    dissipation adt * 0.05;
+ *         update     per cell: d = res / adt; q = qold - d; res = 0 }
+ * and reports rms = sqrt(sum of d^2 / cells) of the second stage.  Boundary
+ * edges are oriented like res_calc's edges: with dx = x1 - x2, dy = y1 - y2
+ * the normal (dy, -dx) points out of the cell.  Every sum has a fixed order,
+ * so with a hierarchical plan a run is bit-reproducible. */
+typedef struct fot_airfoil fot_airfoil;
+typedef struct fot_airfoil_desc {
+  const uint32_t *cell_to_node;  /* cells x 4 nodes, counter-clockwise (original numbering) */
+  uint32_t n_bedges;
+  const uint32_t *bedge_to_node; /* n_bedges x 2: node 1, node 2 */
+  const uint32_t *bedge_to_cell; /* n_bedges */
+  const int32_t *bound;          /* n_bedges: 1 = solid wall, otherwise far field */
+  double qinf[4];                /* free stream (rho, rho u, rho v, rho E) */
+  double cfl;
+} fot_airfoil_desc;
+/* Checks every index against the problem's sizes; renumbers the maps whenever
+ * the problem's numbering changes (fot_reorder, fot_renumber_points, ...). */
+int fot_airfoil_create(fot_problem *p, const fot_airfoil_desc *desc, fot_airfoil **out);
+/* `iterations` solver iterations on `stream`; rms (host, may be NULL) receives
+ * the last iteration's rms after the stream is synchronised. */
+int fot_airfoil_run(fot_airfoil *a, fot_plan *plan, uint32_t iterations, double *rms, void *stream);
+int fot_airfoil_destroy(fot_airfoil *a);
+
 /* ---- batches: many meshes, one persistent launch -------------------------- */
 
 /* Group the plans of several problems into one launch per fot_batch_run.

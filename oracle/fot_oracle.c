@@ -553,6 +553,100 @@ int orc_replay_hier(int loop, int soa, uint32_t n_cells,
   return 0;
 }
 
+/* The Airfoil iteration around res_calc (fot_airfoil_run's kernels in
+ * csrc/airfoil.cu, operation for operation). */
+int orc_airfoil_run(int soa, uint32_t n_edges, const uint32_t *n_points,
+                    const uint32_t *const *maps, void *const *point_data,
+                    const orc_airfoil *A, uint32_t iters, const orc_plan *P,
+                    double *rms) {
+  const double gam = 1.4, gm1 = 0.4, eps = 0.05;
+  const uint32_t nc = n_points[0], nn = n_points[1];
+  double *res = (double *)point_data[0], *q = (double *)point_data[2];
+  double *adt = (double *)point_data[3];
+  const double *x = (const double *)point_data[1];
+  double *qold = (double *)malloc(sizeof(double) * 4 * (size_t)nc);
+  if (!qold) return -1;
+#define AT(n, i, dim, k) (soa ? (size_t)(k) * (n) + (i) : (size_t)(i) * (dim) + (k))
+  double sum = 0.0;
+  for (uint32_t it = 0; it < iters; ++it) {
+    memcpy(qold, q, sizeof(double) * 4 * (size_t)nc);
+    for (int stage = 0; stage < 2; ++stage) {
+      /* adt_calc */
+      for (uint32_t c = 0; c < nc; ++c) {
+        double px[4], py[4];
+        for (int j = 0; j < 4; ++j) {
+          const uint32_t n = A->cell_to_node[4 * (size_t)c + j];
+          px[j] = x[AT(nn, n, 2, 0)];
+          py[j] = x[AT(nn, n, 2, 1)];
+        }
+        const double ri = 1.0 / q[AT(nc, c, 4, 0)];
+        const double u = ri * q[AT(nc, c, 4, 1)], v = ri * q[AT(nc, c, 4, 2)];
+        const double snd = sqrt(gam * gm1 * (ri * q[AT(nc, c, 4, 3)] - 0.5 * (u * u + v * v)));
+        double s = 0.0;
+        for (int j = 0; j < 4; ++j) {
+          const double dx = px[(j + 1) & 3] - px[j];
+          const double dy = py[(j + 1) & 3] - py[j];
+          s += fabs(u * dy - v * dx) + snd * sqrt(dx * dx + dy * dy);
+        }
+        adt[c] = s / A->cfl;
+      }
+      /* res_calc */
+      const int rc = P ? orc_replay_hier(ORC_RES_CALC, soa, n_edges, n_points, maps,
+                                         point_data, NULL, 1, P)
+                       : orc_loop_serial(ORC_RES_CALC, soa, n_edges, n_points, maps,
+                                         point_data, NULL, 1);
+      if (rc) {
+        free(qold);
+        return rc;
+      }
+      /* bres_calc */
+      for (uint32_t e = 0; e < A->n_bedges; ++e) {
+        const uint32_t c = A->bedge_to_cell[e];
+        const uint32_t n1 = A->bedge_to_node[2 * (size_t)e], n2 = A->bedge_to_node[2 * (size_t)e + 1];
+        const double dx = x[AT(nn, n1, 2, 0)] - x[AT(nn, n2, 2, 0)];
+        const double dy = x[AT(nn, n1, 2, 1)] - x[AT(nn, n2, 2, 1)];
+        double q1[4];
+        for (int k = 0; k < 4; ++k) q1[k] = q[AT(nc, c, 4, k)];
+        const double ri = 1.0 / q1[0];
+        const double p1 = gm1 * (q1[3] - 0.5 * ri * (q1[1] * q1[1] + q1[2] * q1[2]));
+        double *r0 = &res[AT(nc, c, 4, 0)], *r1 = &res[AT(nc, c, 4, 1)];
+        double *r2 = &res[AT(nc, c, 4, 2)], *r3 = &res[AT(nc, c, 4, 3)];
+        if (A->bound[e] == 1) {
+          *r1 += p1 * dy;
+          *r2 += -p1 * dx;
+        } else {
+          const double *qi = A->qinf;
+          const double vol1 = ri * (q1[1] * dy - q1[2] * dx);
+          const double ri2 = 1.0 / qi[0];
+          const double p2 = gm1 * (qi[3] - 0.5 * ri2 * (qi[1] * qi[1] + qi[2] * qi[2]));
+          const double vol2 = ri2 * (qi[1] * dy - qi[2] * dx);
+          const double mu = adt[c] * eps;
+          *r0 += 0.5 * (vol1 * q1[0] + vol2 * qi[0]) + mu * (q1[0] - qi[0]);
+          *r1 += 0.5 * (vol1 * q1[1] + p1 * dy + vol2 * qi[1] + p2 * dy) + mu * (q1[1] - qi[1]);
+          *r2 += 0.5 * (vol1 * q1[2] - p1 * dx + vol2 * qi[2] - p2 * dx) + mu * (q1[2] - qi[2]);
+          *r3 += 0.5 * (vol1 * (q1[3] + p1) + vol2 * (qi[3] + p2)) + mu * (q1[3] - qi[3]);
+        }
+      }
+      /* update */
+      sum = 0.0;
+      for (uint32_t c = 0; c < nc; ++c) {
+        const double adti = 1.0 / adt[c];
+        for (int k = 0; k < 4; ++k) {
+          const size_t o = AT(nc, c, 4, k);
+          const double del = adti * res[o];
+          q[o] = qold[o] - del;
+          res[o] = 0.0;
+          sum += del * del;
+        }
+      }
+    }
+  }
+#undef AT
+  if (rms) *rms = sqrt(sum / (double)nc);
+  free(qold);
+  return 0;
+}
+
 int orc_is_permutation(const uint32_t *perm, uint32_t n) {
   unsigned char *seen = (unsigned char *)calloc(n ? n : 1, 1);
   int ok = 1;

@@ -81,6 +81,28 @@ int orc_replay_hier(int loop, int soa, uint32_t n_cells,
                     void *const *point_data, void *const *cell_data,
                     uint32_t iters, const orc_plan *plan);
 
+/* The Airfoil solver iteration the engine runs around res_calc
+ * (fot_airfoil_run; not part of the reference, which drives res_calc alone):
+ * save_soln, then twice { adt_calc, res_calc, bres_calc, update }, with the
+ * same operations in the same order as the engine's kernels.  point_data are
+ * res_calc's (res 0, x 1, q 2, adt 3) in the problem layout; res_calc runs in
+ * serial edge order when P is NULL, else replays P's colour order.  The
+ * boundary edges add in edge order; rms = sqrt(sum of squared updates /
+ * cells) of the last iteration's second stage, summed in cell order. */
+typedef struct orc_airfoil {
+  const uint32_t *cell_to_node;  /* n_cells x 4 */
+  uint32_t n_bedges;
+  const uint32_t *bedge_to_node; /* n_bedges x 2 */
+  const uint32_t *bedge_to_cell;
+  const int32_t *bound;
+  double qinf[4];
+  double cfl;
+} orc_airfoil;
+int orc_airfoil_run(int soa, uint32_t n_edges, const uint32_t *n_points,
+                    const uint32_t *const *maps, void *const *point_data,
+                    const orc_airfoil *A, uint32_t iters, const orc_plan *P,
+                    double *rms);
+
 /* Exact checks of a plan against mapping 0 (n_cells x mesh_dim) and the block
  * size.  Returns 0 when valid, otherwise a nonzero code naming the first
  * failed check (see fot_oracle.c) and writes a message into err. */

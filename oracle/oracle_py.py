@@ -141,6 +141,38 @@ def replay_hier(md, plan: dict, iters: int = 1):
     return pd, cd
 
 
+class OrcAirfoil(C.Structure):
+    _fields_ = [("cell_to_node", u32p), ("n_bedges", C.c_uint32), ("bedge_to_node", u32p),
+                ("bedge_to_cell", u32p), ("bound", C.POINTER(C.c_int32)),
+                ("qinf", C.c_double * 4), ("cfl", C.c_double)]
+
+
+def airfoil(md, extras: dict, iters: int = 1, plan: Optional[dict] = None):
+    """The Airfoil iteration around res_calc (orc_airfoil_run): returns
+    (point_data after `iters` iterations, rms of the last one).  res_calc
+    runs in serial edge order, or replays `plan` (an exported plan, cell_id
+    relative to md's cells)."""
+    pd, cd = _copies(md)
+    a = _Args(md, pd, cd)
+    keep = [np.ascontiguousarray(extras["cell_to_node"], dtype=np.uint32),
+            np.ascontiguousarray(extras["bedge_to_node"], dtype=np.uint32),
+            np.ascontiguousarray(extras["bedge_to_cell"], dtype=np.uint32),
+            np.ascontiguousarray(extras["bound"], dtype=np.int32)]
+    A = OrcAirfoil(keep[0].ctypes.data_as(u32p), len(keep[2]), keep[1].ctypes.data_as(u32p),
+                   keep[2].ctypes.data_as(u32p), keep[3].ctypes.data_as(C.POINTER(C.c_int32)),
+                   (C.c_double * 4)(*[float(v) for v in extras["qinf"]]), float(extras["cfl"]))
+    P = None
+    if plan is not None:
+        p, pkeep = _orc_plan(plan)
+        P = C.byref(p)
+    rms = C.c_double()
+    rc = orc().orc_airfoil_run(int(md.layout == "soa"), md.n_cells, a.n_points, a.map_ptrs,
+                               a.pd_ptrs, C.byref(A), iters, P, C.byref(rms))
+    if rc:
+        raise RuntimeError(f"orc_airfoil_run failed: {rc}")
+    return pd, rms.value
+
+
 def check_plan(plan: dict, map0: np.ndarray, n_points0: int, block_size: int):
     """Returns (code, message); code 0 means the plan is valid."""
     p, keep = _orc_plan(plan)
