@@ -23,8 +23,8 @@ Each function returns a dict for one key of bench.py's JSON line:
   and mini_aero 128^3, beside the reference's host builder
   (HierarchicalColourMemory, colouring.hpp:44-147) timed on the same mesh;
 * ``airfoil_1000``   the Airfoil solver iteration around res_calc (save_soln,
-  then twice adt_calc, res_calc, bres_calc, update: fot_airfoil_run) on the
-  1000 x 1000 mesh, with res_calc through the best atomic plan and through a
+  then twice adt_calc, res_calc, bres_calc, update: fot_airfoil_run, whose
+  per-cell loops run fused) on the 1000 x 1000 mesh, with res_calc through the best atomic plan and through a
   coloured one: time per iteration, GB/s of the iteration's unique bytes, and
   the share of res_calc in it.
 """
@@ -185,19 +185,19 @@ def atomic_spread(md: mg.MeshData, cand: T.Candidate, runs: int = 6) -> dict:
 
 
 def airfoil_unique_bytes(md: mg.MeshData, ex: dict) -> int:
-    """Algorithmic bytes of one Airfoil iteration: save_soln (q read, qold
-    written), and twice adt_calc (cell->node map, node coordinates, q, adt
-    written), res_calc (its unique bytes), bres_calc (boundary maps and
-    flags, the boundary cells' q, adt, res read and written) and update
-    (qold, q written, res read and written, adt)."""
+    """Algorithmic bytes of one Airfoil iteration in its fused form: twice
+    res_calc (its unique bytes) and bres_calc (boundary maps and flags, the
+    boundary cells' q, adt and res), the stage-1 cell pass (update + adt_calc:
+    qold, res and adt read, q written, res zeroed, the cell->node map and
+    node coordinates read, adt written) and the stage-2 pass that also saves
+    qold for the next iteration."""
     nc, nn = md.n_points[0], md.n_points[1]
     nb = len(ex["bedge_to_cell"])
     nbc = len(np.unique(ex["bedge_to_cell"]))
-    save = nc * 64
-    adt = nc * 16 + nn * 16 + nc * 32 + nc * 8
     bres = nb * (8 + 4 + 4) + nbc * (32 + 8 + 64)
-    update = nc * (32 + 32 + 64 + 8)
-    return save + 2 * (adt + md.unique_bytes() + bres + update)
+    adt = nc * 16 + nn * 16 + nc * 8
+    update = nc * (32 + 64 + 8 + 32)
+    return 2 * (md.unique_bytes() + bres) + 2 * (update + adt) + nc * 32
 
 
 def airfoil_1000(peak: float, stream, iters: int = 20) -> dict:

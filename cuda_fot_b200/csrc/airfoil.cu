@@ -21,7 +21,11 @@
 // adt (3) in its current numbering and layout, plus the airfoil's own qold,
 // cell -> 4 nodes, boundary edge -> 2 nodes / 1 cell / bound flag (given in
 // the original numbering and renumbered here whenever the problem's
-// numbering changes).  Every kernel is compiled without multiply-add
+// numbering changes).  The per-cell loops run fused, each cell's values
+// unchanged: update + the next stage's adt_calc in one pass (and between
+// iterations + save_soln), so an iteration is two res_calc runs, two
+// bres_calc launches, two cell passes and the rms reduction.
+// Every kernel is compiled without multiply-add
 // contraction, and every sum has a fixed order: boundary edges are added per
 // cell in increasing edge order (one thread per boundary cell), the rms is a
 // fixed-shape tree.  With a coloured res_calc plan a step is therefore
@@ -59,31 +63,27 @@ __device__ __forceinline__ size_t at(int soa, uint32_t n, uint32_t i, int dim, i
   return soa ? (size_t)k * n + i : (size_t)i * dim + k;
 }
 
-__global__ void __launch_bounds__(kThreads) k_adt_calc(AirfoilDev a) {
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < a.n_cells; c += stride) {
-    const uint4 nd = a.cell_nodes[c];
-    const uint32_t node[4] = {nd.x, nd.y, nd.z, nd.w};
-    double px[4], py[4];
+// adt_calc of cell c from its state q.
+__device__ __forceinline__ double cell_adt(const AirfoilDev &a, uint32_t c, const double (&q)[4]) {
+  const uint4 nd = a.cell_nodes[c];
+  const uint32_t node[4] = {nd.x, nd.y, nd.z, nd.w};
+  double px[4], py[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      px[j] = a.x[at(a.soa, a.n_nodes, node[j], 2, 0)];
-      py[j] = a.x[at(a.soa, a.n_nodes, node[j], 2, 1)];
-    }
-    const double q0 = a.q[at(a.soa, a.n_cells, c, 4, 0)], q1 = a.q[at(a.soa, a.n_cells, c, 4, 1)];
-    const double q2 = a.q[at(a.soa, a.n_cells, c, 4, 2)], q3 = a.q[at(a.soa, a.n_cells, c, 4, 3)];
-    const double ri = 1.0 / q0;
-    const double u = ri * q1, v = ri * q2;
-    const double snd = sqrt(kGam * kGm1 * (ri * q3 - 0.5 * (u * u + v * v)));
-    double s = 0.0;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const double dx = px[(j + 1) & 3] - px[j];
-      const double dy = py[(j + 1) & 3] - py[j];
-      s += fabs(u * dy - v * dx) + snd * sqrt(dx * dx + dy * dy);
-    }
-    a.adt[c] = s / a.cfl;
+  for (int j = 0; j < 4; ++j) {
+    px[j] = a.x[at(a.soa, a.n_nodes, node[j], 2, 0)];
+    py[j] = a.x[at(a.soa, a.n_nodes, node[j], 2, 1)];
   }
+  const double ri = 1.0 / q[0];
+  const double u = ri * q[1], v = ri * q[2];
+  const double snd = sqrt(kGam * kGm1 * (ri * q[3] - 0.5 * (u * u + v * v)));
+  double s = 0.0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const double dx = px[(j + 1) & 3] - px[j];
+    const double dy = py[(j + 1) & 3] - py[j];
+    s += fabs(u * dy - v * dx) + snd * sqrt(dx * dx + dy * dy);
+  }
+  return s / a.cfl;
 }
 
 // One thread per boundary cell: its boundary edges in increasing edge order.
@@ -138,23 +138,42 @@ __device__ __forceinline__ double block_sum(double v, double *smem) {
   return s;
 }
 
-__global__ void __launch_bounds__(kThreads) k_update(AirfoilDev a, double *partial) {
+// The per-cell loops of the iteration, fused (each cell's values are the
+// same as loop by loop): UPDATE (q = qold - res / adt, res = 0, squared
+// updates summed per CTA in a fixed order into partial[]), then SAVE
+// (qold = q: save_soln of the next iteration) and ADT (adt_calc on the new q).
+template <bool UPDATE, bool SAVE, bool ADT>
+__global__ void __launch_bounds__(kThreads) k_cells(AirfoilDev a, double *partial) {
   __shared__ double smem[kThreads / 32];
   double sum = 0.0;
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < a.n_cells; c += stride) {
-    const double adti = 1.0 / a.adt[c];
+    double q[4];
+    if constexpr (UPDATE) {
+      const double adti = 1.0 / a.adt[c];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const size_t o = at(a.soa, a.n_cells, c, 4, k);
-      const double del = adti * a.res[o];
-      a.q[o] = a.qold[o] - del;
-      a.res[o] = 0.0;
-      sum += del * del;
+      for (int k = 0; k < 4; ++k) {
+        const size_t o = at(a.soa, a.n_cells, c, 4, k);
+        const double del = adti * a.res[o];
+        q[k] = a.qold[o] - del;
+        a.q[o] = q[k];
+        a.res[o] = 0.0;
+        sum += del * del;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) q[k] = a.q[at(a.soa, a.n_cells, c, 4, k)];
     }
+    if constexpr (SAVE) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) a.qold[at(a.soa, a.n_cells, c, 4, k)] = q[k];
+    }
+    if constexpr (ADT) a.adt[c] = cell_adt(a, c, q);
   }
-  const double s = block_sum(sum, smem);
-  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  if constexpr (UPDATE) {
+    const double s = block_sum(sum, smem);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  }
 }
 
 __global__ void __launch_bounds__(kThreads) k_rms(const double *partial, uint32_t n_partial,
@@ -319,21 +338,27 @@ int fot_airfoil_run(fot_airfoil *a, fot_plan *plan, uint32_t iterations, double 
   d.cfl = a->cfl;
   const uint32_t ctas = update_ctas(a->n_cells);
   const uint32_t bctas = (a->n_bcells + kThreads - 1) / kThreads;
-  const size_t qbytes = (size_t)a->n_cells * 4 * sizeof(double);
+  double *part = a->partial.as<double>();
+  // save_soln + adt_calc of the first stage; afterwards each update carries
+  // the next stage's adt_calc (and, between iterations, save_soln)
+  k_cells<false, true, true><<<ctas, kThreads, 0, st>>>(d, part);
+  FOT_CUDA(cudaGetLastError());
   for (uint32_t it = 0; it < iterations; ++it) {
-    FOT_CUDA(cudaMemcpyAsync(d.qold, d.q, qbytes, cudaMemcpyDeviceToDevice, st));
     for (int stage = 0; stage < 2; ++stage) {
-      k_adt_calc<<<ctas, kThreads, 0, st>>>(d);
-      FOT_CUDA(cudaGetLastError());
       FOT_TRY(fot_run(p, plan, 1, stream));
       if (bctas) {
         k_bres_calc<<<bctas, kThreads, 0, st>>>(d);
         FOT_CUDA(cudaGetLastError());
       }
-      k_update<<<ctas, kThreads, 0, st>>>(d, a->partial.as<double>());
+      if (stage == 0)
+        k_cells<true, false, true><<<ctas, kThreads, 0, st>>>(d, part);
+      else if (it + 1 < iterations)
+        k_cells<true, true, true><<<ctas, kThreads, 0, st>>>(d, part);
+      else
+        k_cells<true, false, false><<<ctas, kThreads, 0, st>>>(d, part);
       FOT_CUDA(cudaGetLastError());
     }
-    k_rms<<<1, kThreads, 0, st>>>(a->partial.as<double>(), ctas, a->n_cells, a->rms.as<double>());
+    k_rms<<<1, kThreads, 0, st>>>(part, ctas, a->n_cells, a->rms.as<double>());
     FOT_CUDA(cudaGetLastError());
   }
   if (rms) {

@@ -173,8 +173,6 @@ fot::HierPlanDev fot_plan::dev(uint32_t iterations) const {
   P.n_shared = n_shared_points;
   P.tiles_on = 1;
   P.ctl = ctl.as<Ctl>();
-  // the direct split kernel's CTAs resident at once (its prefetch distance)
-  if ((variant & kVariantSplit) && !(variant & kVariantPipe)) P.ahead = (uint32_t)(per_sm * device_sm_count());
   return P;
 }
 

@@ -89,10 +89,6 @@ struct HierPlanDev {
   // per launch: tiles run (0: combine only), the buffer they fill, whether
   // the other buffer (previous iteration) is combined, CTAs doing that
   uint32_t tiles_on, put_buf, comb_on, comb_ctas;
-  // direct split kernel: CTAs resident at once; each tile CTA prefetches the
-  // plan data and direct data of the tile this many places later into L2
-  // (0: no prefetch)
-  uint32_t ahead;
 };
 
 // Direct (cell) data of one cell: SOA with stride n_cells.
@@ -255,27 +251,33 @@ __device__ __forceinline__ void prefetch_l2(const void *p) {
 
 // Prefetch cell c's mapping rows and direct data (every component of every
 // cell dataset, SOA) into L2; one instruction per array covers a warp's 32
-// consecutive cells.
+// consecutive cells.  Straight-line code: the loops over the loop's cell
+// datasets and their (at most kMaxPrefetchDim) components are unrolled.
+constexpr uint32_t kMaxPrefetchDim = 12;
 template <class L> __device__ __forceinline__ void prefetch_cell(const LoopData &d, uint32_t c) {
   prefetch_l2(d.map[0] + (size_t)c * L::kDim);
   if constexpr (L::kHasClass1) prefetch_l2(d.map[1] + (size_t)c * L::kDim);
-  for (uint32_t j = 0; j < d.n_cell_sets; ++j) {
+#pragma unroll
+  for (int j = 0; j < L::kNumDirect; ++j) {
     const char *b = static_cast<const char *>(d.cell[j]) + (size_t)c * d.cell_size[j];
     const size_t stride = (size_t)d.n_cells * d.cell_size[j];
-    for (uint32_t k = 0; k < d.cell_dim[j]; ++k) prefetch_l2(b + k * stride);
+#pragma unroll
+    for (uint32_t k = 0; k < kMaxPrefetchDim; ++k)
+      if (k < d.cell_dim[j]) prefetch_l2(b + k * stride);
   }
 }
 
 // Persistent grid-stride loop over 32-cell chunks, one chunk per warp at a
-// time; with L::kAtomicPrefetch each warp first prefetches the chunk it will
-// take next, so that its mapping rows and direct data come from L2 then.
+// time; with L::kAtomicPrefetch, in the SOA form, each warp first prefetches
+// the chunk it will take next, so that its mapping rows and direct data come
+// from L2 then.
 template <class L, bool SOA, bool AGG>
 __global__ void __launch_bounds__(256, L::kAtomicMinBlocks) k_atomic(LoopData d) {
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t lane = threadIdx.x & 31u;
   for (uint32_t base = warp * 32u; base < d.n_cells; base += n_warps * 32u) {
-    if constexpr (L::kAtomicPrefetch) {
+    if constexpr (L::kAtomicPrefetch && SOA) {
       const uint32_t next = base + n_warps * 32u + lane;
       if (next < d.n_cells) prefetch_cell<L>(d, next);
     }

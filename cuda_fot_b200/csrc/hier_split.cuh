@@ -143,21 +143,6 @@ __device__ __forceinline__ void split_writeback(const LoopData &d, const HierPla
 // replay's order, bit for bit); then each written point's sum goes out (RED
 // for private points, the slot for shared ones).  The tile header (start,
 // cells | colours << 16, written points, their offset) is one 16-byte load.
-#ifndef FOT_DSPLIT_PREFETCH
-#define FOT_DSPLIT_PREFETCH 0
-#endif
-
-// Prefetch into L2 what the tile at position `pos` of a later CTA reads
-// besides its points' rows: its mapping rows, local indices, thread colour
-// and direct data.
-template <class L>
-__device__ __forceinline__ void prefetch_tile_cell(const LoopData &d, const HierPlanDev &P, uint32_t pos) {
-  prefetch_cell<L>(d, pos);
-#pragma unroll
-  for (int q = 0; q < L::kDim; ++q) prefetch_l2(P.lidx[0] + (size_t)q * d.n_cells + pos);
-  prefetch_l2(P.tcol + pos);
-}
-
 template <class L, int T> constexpr int dsplit_min_blocks() {
   return (65536 / (T * L::kDirectRegCap)) > 0 ? 65536 / (T * L::kDirectRegCap) : 1;
 }
@@ -185,11 +170,6 @@ __global__ void __launch_bounds__(T, dsplit_min_blocks<L, T>()) k_hier_dsplit(Lo
   }
   const uint4 h = __ldg(P.tile_hdr + blockIdx.x);
   const uint32_t start = h.x, ncell = h.y & 0xFFFFu, ntcol = h.y >> 16, n0 = h.z, poff = h.w;
-#if FOT_DSPLIT_PREFETCH
-  // the tile a resident wave later (scheduled about when this one finishes)
-  const bool pf = P.ahead != 0 && blockIdx.x + P.ahead < n_tiles;
-  const uint4 hn = pf ? __ldg(P.tile_hdr + blockIdx.x + P.ahead) : make_uint4(0, 0, 0, 0);
-#endif
   for (uint32_t e = tid; e < n0 * K; e += T) acc[e] = out_t(0);
   // this thread's first written point (issued early; used after the sums)
   uint32_t p_first = 0, ws_first = 0;
@@ -218,9 +198,6 @@ __global__ void __launch_bounds__(T, dsplit_min_blocks<L, T>()) k_hier_dsplit(Lo
     Direct dir{d.cell, pos, d.n_cells};
     L::cell(rows, dir, v);
   }
-#if FOT_DSPLIT_PREFETCH
-  if (pf && tid < (hn.y & 0xFFFFu)) prefetch_tile_cell<L>(d, P, hn.x + tid);
-#endif
   __syncthreads();  // the sums are zeroed
   for (uint32_t col = 0; col < ntcol; ++col) {
     if (my_col == col) {
