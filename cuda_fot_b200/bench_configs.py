@@ -25,8 +25,9 @@ Each function returns a dict for one key of bench.py's JSON line:
 * ``airfoil_1000``   the Airfoil solver iteration around res_calc (save_soln,
   then twice adt_calc, res_calc, bres_calc, update: fot_airfoil_run, whose
   per-cell loops run fused) on the 1000 x 1000 mesh, with res_calc through the best atomic plan and through a
-  coloured one: time per iteration, GB/s of the iteration's unique bytes, and
-  the share of res_calc in it.
+  coloured one: time per iteration (launched call by call, and replayed as
+  one CUDA graph of the time loop), GB/s of the iteration's unique bytes,
+  and the share of res_calc in it.
 """
 from __future__ import annotations
 
@@ -200,6 +201,31 @@ def airfoil_unique_bytes(md: mg.MeshData, ex: dict) -> int:
     return 2 * (md.unique_bytes() + bres) + 2 * (update + adt) + nc * 32
 
 
+def airfoil_setup(md: mg.MeshData, ex: dict, cand: T.Candidate):
+    """A problem holding md, ordered / partitioned on the GPU as the
+    candidate says, the candidate's res_calc plan and the Airfoil step on it
+    (its maps given in md's numbering)."""
+    p = F.Problem.from_mesh(md)
+    if cand.order is not None:
+        p.reorder(T.ORDERS[cand.order], seed=1)
+    flags = 0
+    if cand.partition:
+        p.partition(cand.partition)
+        p.reorder_to_partition()
+        p.renumber_points()
+        flags |= F.PLAN_USE_PARTITION
+    if cand.layout != md.layout:
+        p.set_layout(cand.layout)
+    if cand.direct:
+        flags |= F.PLAN_DIRECT_READS
+    if cand.exec == "atomic" and not cand.aggregate:
+        flags |= F.PLAN_NO_AGGREGATE
+    plan = p.plan(T.EXECS[cand.exec], cand.block, flags)
+    af = F.Airfoil(p, ex["cell_to_node"], ex["bedge_to_node"], ex["bedge_to_cell"],
+                   ex["bound"], ex["qinf"], ex["cfl"])
+    return p, plan, af
+
+
 def airfoil_1000(peak: float, stream, iters: int = 20) -> dict:
     import torch
     md = mg.res_calc(1000, 1000, 1)
@@ -208,20 +234,9 @@ def airfoil_1000(peak: float, stream, iters: int = 20) -> dict:
     out = {"workload": "Airfoil iteration: save_soln + 2 x (adt_calc, res_calc, bres_calc, update) "
                        "on res_calc 1000x1000 (1,998,000 edges, 4,000 boundary edges), FP64",
            "unique_bytes_per_iteration": ub}
-    for name, (order, part, layout, exec_, block, flags) in (
-            ("atomic", ("rcm", 0, "soa", F.EXEC_ATOMIC, 256, F.PLAN_NO_AGGREGATE)),
-            ("coloured", ("rcm", 256, "aos", F.EXEC_HIER, 256, F.PLAN_USE_PARTITION))):
-        p = F.Problem.from_mesh(md)
-        p.reorder(T.ORDERS[order], seed=1)
-        if part:
-            p.partition(part)
-            p.reorder_to_partition()
-            p.renumber_points()
-        if layout != md.layout:
-            p.set_layout(layout)
-        plan = p.plan(exec_, block, flags)
-        af = F.Airfoil(p, ex["cell_to_node"], ex["bedge_to_node"], ex["bedge_to_cell"],
-                       ex["bound"], ex["qinf"], ex["cfl"])
+    for name, cand in (("atomic", T.Candidate("rcm", 0, "atomic", 256, aggregate=False, layout="soa")),
+                       ("coloured", T.Candidate("rcm", 256, "hier", 256))):
+        p, plan, af = airfoil_setup(md, ex, cand)
         af.run(plan, 3, stream, rms=False)
         p.sync(stream)
         a = torch.cuda.Event(enable_timing=True)
@@ -232,11 +247,19 @@ def airfoil_1000(peak: float, stream, iters: int = 20) -> dict:
         b.synchronize()
         secs = a.elapsed_time(b) / 1e3 / iters
         rms = af.run(plan, 1, stream)
+        g = af.graph(plan, iters, stream)
+        g.launch(stream)
+        p.sync(stream)
+        a.record(stream)
+        g.launch(stream)
+        b.record(stream)
+        b.synchronize()
+        gsecs = a.elapsed_time(b) / 1e3 / iters
+        del g
         loop_s = T.time_plan(p, plan, iters, 3, stream)
-        label = f"{order}{'+part%d' % part if part else ''}/" + \
-                ("atomic-plain/256" if exec_ == F.EXEC_ATOMIC else f"hier/{block}") + \
-                ("@soa" if layout == "soa" else "")
-        out[name] = {"res_calc_plan": label, "us_per_iteration": round(secs * 1e6, 2),
+        out[name] = {"res_calc_plan": cand.label(), "us_per_iteration": round(secs * 1e6, 2),
+                     "graph_us_per_iteration": round(gsecs * 1e6, 2),
+                     "graph_gbs": round(ub / gsecs / 1e9, 1),
                      "gbs": round(ub / secs / 1e9, 1), "frac": round(_frac(ub / secs / 1e9, peak), 4),
                      "res_calc_share": round(2 * loop_s / secs, 3), "rms_after": rms}
         del af, plan, p

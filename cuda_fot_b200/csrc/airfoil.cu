@@ -42,7 +42,11 @@ namespace {
 
 constexpr double kGam = 1.4, kGm1 = 0.4, kEps = 0.05; // gm1 and eps as res_calc_func.hpp
 constexpr uint32_t kThreads = 256;
-constexpr uint32_t kMaxUpdateCtas = 1184;
+#ifndef FOT_AIRFOIL_MAX_CTAS
+#define FOT_AIRFOIL_MAX_CTAS 1184
+#endif
+// CTAs of a cell pass (grid-stride beyond); the rms sums one partial per CTA
+constexpr uint32_t kMaxUpdateCtas = FOT_AIRFOIL_MAX_CTAS;
 
 struct AirfoilDev {
   const double *x;
@@ -291,8 +295,10 @@ int fot_airfoil_create(fot_problem *p, const fot_airfoil_desc *desc, fot_airfoil
   a->cfl = desc->cfl;
   int rc = airfoil_renumber(a);
   if (rc == FOT_OK) rc = a->qold.alloc((size_t)n_cells * 4 * sizeof(double));
-  if (rc == FOT_OK) rc = a->partial.alloc(kMaxUpdateCtas * sizeof(double));
+  if (rc == FOT_OK) rc = a->partial.alloc(update_ctas(n_cells) * sizeof(double));
   if (rc == FOT_OK) rc = a->rms.alloc(sizeof(double));
+  if (rc == FOT_OK && cudaMemset(a->rms.ptr, 0, sizeof(double)) != cudaSuccess)
+    rc = fail(FOT_ERR_CUDA, "cudaMemset failed");
   if (rc != FOT_OK) {
     delete a;
     return rc;
@@ -312,13 +318,13 @@ int fot_airfoil_destroy(fot_airfoil *a) {
   return FOT_OK;
 }
 
-int fot_airfoil_run(fot_airfoil *a, fot_plan *plan, uint32_t iterations, double *rms, void *stream) {
-  if (!a || !plan) return fail(FOT_ERR_ARG, "null argument");
+} // extern "C"
+
+namespace {
+
+// Launch `iterations` solver iterations on st (no synchronisation).
+int airfoil_enqueue(fot_airfoil *a, fot_plan *plan, uint32_t iterations, cudaStream_t st) {
   fot_problem *p = a->prob;
-  if (!p) return fail(FOT_ERR_STATE, "the airfoil's problem was destroyed");
-  if (iterations == 0) return FOT_OK;
-  if (a->version != p->version) FOT_TRY(airfoil_renumber(a));
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   AirfoilDev d{};
   d.x = static_cast<const double *>(p->point[1].ptr);
   d.q = static_cast<double *>(p->point[2].ptr);
@@ -345,7 +351,7 @@ int fot_airfoil_run(fot_airfoil *a, fot_plan *plan, uint32_t iterations, double 
   FOT_CUDA(cudaGetLastError());
   for (uint32_t it = 0; it < iterations; ++it) {
     for (int stage = 0; stage < 2; ++stage) {
-      FOT_TRY(fot_run(p, plan, 1, stream));
+      FOT_TRY(fot_run(p, plan, 1, st));
       if (bctas) {
         k_bres_calc<<<bctas, kThreads, 0, st>>>(d);
         FOT_CUDA(cudaGetLastError());
@@ -361,10 +367,60 @@ int fot_airfoil_run(fot_airfoil *a, fot_plan *plan, uint32_t iterations, double 
     k_rms<<<1, kThreads, 0, st>>>(part, ctas, a->n_cells, a->rms.as<double>());
     FOT_CUDA(cudaGetLastError());
   }
+  return FOT_OK;
+}
+
+int airfoil_ready(fot_airfoil *a, fot_plan *plan) {
+  if (!a || !plan) return fail(FOT_ERR_ARG, "null argument");
+  if (!a->prob) return fail(FOT_ERR_STATE, "the airfoil's problem was destroyed");
+  if (plan->prob != a->prob) return fail(FOT_ERR_STATE, "plan belongs to another (or a destroyed) problem");
+  if (a->version != a->prob->version) FOT_TRY(airfoil_renumber(a));
+  return FOT_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int fot_airfoil_run(fot_airfoil *a, fot_plan *plan, uint32_t iterations, double *rms, void *stream) {
+  FOT_TRY(airfoil_ready(a, plan));
+  if (iterations == 0) return FOT_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  FOT_TRY(airfoil_enqueue(a, plan, iterations, st));
   if (rms) {
     FOT_CUDA(cudaMemcpyAsync(rms, a->rms.ptr, sizeof(double), cudaMemcpyDeviceToHost, st));
     FOT_CUDA(cudaStreamSynchronize(st));
   }
+  return FOT_OK;
+}
+
+int fot_airfoil_graph_create(fot_airfoil *a, fot_plan *plan, uint32_t iterations, void *stream,
+                             fot_graph **out) {
+  if (!out) return fail(FOT_ERR_ARG, "null argument");
+  *out = nullptr;
+  FOT_TRY(airfoil_ready(a, plan));
+  if (iterations == 0) return fail(FOT_ERR_ARG, "a graph of zero iterations");
+  struct Ctx {
+    fot_airfoil *a;
+    fot_plan *plan;
+    uint32_t iterations;
+  } ctx{a, plan, iterations};
+  auto enqueue = [](void *c, cudaStream_t st) {
+    const Ctx *x = static_cast<const Ctx *>(c);
+    return airfoil_enqueue(x->a, x->plan, x->iterations, st);
+  };
+  FOT_TRY(capture_graph(static_cast<cudaStream_t>(stream), enqueue, &ctx, out));
+  (*out)->prob = a->prob;
+  (*out)->plan = plan;
+  (*out)->ctl = plan->ctl.as<Ctl>();
+  return FOT_OK;
+}
+
+int fot_airfoil_get_rms(fot_airfoil *a, double *rms, void *stream) {
+  if (!a || !rms) return fail(FOT_ERR_ARG, "null argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  FOT_CUDA(cudaMemcpyAsync(rms, a->rms.ptr, sizeof(double), cudaMemcpyDeviceToHost, st));
+  FOT_CUDA(cudaStreamSynchronize(st));
   return FOT_OK;
 }
 

@@ -642,34 +642,19 @@ int fot_graph_create(fot_problem *p, fot_plan *plan, uint32_t iterations, void *
                      fot_graph **out) {
   if (!p || !plan || !out) return fail(FOT_ERR_ARG, "null argument");
   *out = nullptr;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  cudaStream_t cap = st;
-  bool own = false;
-  if (!cap) {
-    FOT_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
-    own = true;
-  }
-  FOT_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-  const int rc = run_plan(p, plan, iterations, cap);
-  cudaGraph_t graph = nullptr;
-  const cudaError_t e = cudaStreamEndCapture(cap, &graph);
-  if (own) cudaStreamDestroy(cap);
-  if (rc != FOT_OK) {
-    if (graph) cudaGraphDestroy(graph);
-    return rc;
-  }
-  if (e != cudaSuccess) return fail(FOT_ERR_CUDA, "stream capture: %s", cudaGetErrorString(e));
-  auto *g = new fot_graph();
-  g->graph = graph;
-  g->prob = p;
-  g->plan = plan;
-  g->ctl = plan->ctl.as<Ctl>();
-  const cudaError_t e2 = cudaGraphInstantiate(&g->exec, graph, 0);
-  if (e2 != cudaSuccess) {
-    delete g;
-    return fail(FOT_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e2));
-  }
-  *out = g;
+  struct Ctx {
+    fot_problem *p;
+    fot_plan *plan;
+    uint32_t iterations;
+  } ctx{p, plan, iterations};
+  auto enqueue = [](void *c, cudaStream_t st) {
+    const Ctx *x = static_cast<const Ctx *>(c);
+    return run_plan(x->p, x->plan, x->iterations, st);
+  };
+  FOT_TRY(capture_graph(static_cast<cudaStream_t>(stream), enqueue, &ctx, out));
+  (*out)->prob = p;
+  (*out)->plan = plan;
+  (*out)->ctl = plan->ctl.as<Ctl>();
   return FOT_OK;
 }
 
@@ -686,3 +671,41 @@ int fot_graph_destroy(fot_graph *g) {
 }
 
 } // extern "C"
+
+namespace fot {
+
+int capture_graph(cudaStream_t st, int (*enqueue)(void *ctx, cudaStream_t st), void *ctx,
+                  fot_graph **out) {
+  *out = nullptr;
+  cudaStream_t cap = st;
+  bool own = false;
+  if (!cap) {
+    FOT_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    own = true;
+  }
+  const cudaError_t b = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+  if (b != cudaSuccess) {
+    if (own) cudaStreamDestroy(cap);
+    return fail(FOT_ERR_CUDA, "begin capture: %s", cudaGetErrorString(b));
+  }
+  const int rc = enqueue(ctx, cap);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(cap, &graph);
+  if (own) cudaStreamDestroy(cap);
+  if (rc != FOT_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(FOT_ERR_CUDA, "stream capture: %s", cudaGetErrorString(e));
+  auto *g = new fot_graph();
+  g->graph = graph;
+  const cudaError_t e2 = cudaGraphInstantiate(&g->exec, graph, 0);
+  if (e2 != cudaSuccess) {
+    delete g;
+    return fail(FOT_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e2));
+  }
+  *out = g;
+  return FOT_OK;
+}
+
+} // namespace fot

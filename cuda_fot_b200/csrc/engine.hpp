@@ -111,6 +111,13 @@ struct fot_problem {
 // An Airfoil step whose problem is being destroyed (fails from now on).
 void fot_airfoil_detach(struct fot_airfoil *a);
 
+namespace fot {
+// Capture into a new fot_graph what enqueue(ctx, stream) launches (on a
+// private non-blocking stream when st is the legacy default stream).
+int capture_graph(cudaStream_t st, int (*enqueue)(void *ctx, cudaStream_t st), void *ctx,
+                  fot_graph **out);
+} // namespace fot
+
 struct fot_plan {
   fot_problem *prob = nullptr;
   uint64_t version = 0;

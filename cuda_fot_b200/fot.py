@@ -248,9 +248,38 @@ class Airfoil:
                                     C.byref(out) if rms else None, _stream_ptr(stream)))
         return out.value if rms else None
 
+    def graph(self, plan: Plan, iterations: int, stream=None) -> "AirfoilGraph":
+        """`iterations` solver iterations captured as one CUDA graph."""
+        return AirfoilGraph(self, plan, iterations, stream)
+
+    def rms(self, stream=None) -> float:
+        """The last iteration's rms (synchronises the stream)."""
+        out = C.c_double()
+        _check(_lib.fot_airfoil_get_rms(self._h, C.byref(out), _stream_ptr(stream)))
+        return out.value
+
     def __del__(self):
         if getattr(self, "_h", None) is not None and self._h.value:
             _lib.fot_airfoil_destroy(self._h)
+            self._h = None
+
+
+class AirfoilGraph:
+    """Airfoil solver iterations captured as one CUDA graph
+    (fot_airfoil_graph_create); launch() replays them."""
+
+    def __init__(self, airfoil: Airfoil, plan: Plan, iterations: int, stream=None):
+        self.airfoil, self.plan = airfoil, plan
+        self._h = C.c_void_p()
+        _check(_lib.fot_airfoil_graph_create(airfoil._h, plan._h, C.c_uint32(iterations),
+                                             _stream_ptr(stream), C.byref(self._h)))
+
+    def launch(self, stream=None) -> None:
+        _check(_lib.fot_graph_launch(self._h, _stream_ptr(stream)))
+
+    def __del__(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.fot_graph_destroy(self._h)
             self._h = None
 
 

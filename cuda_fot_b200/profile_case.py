@@ -5,7 +5,9 @@
 
 Builds the mesh and the plan, then calls Plan.run(1) `--launches` times, so a
 profiler can skip the first launches (-s) and capture one to three (-c) of the
-same kernel.  Plan labels are those of cuda_fot_b200.tune.Candidate.label():
+same kernel.  With --airfoil (res_calc only) it runs that many Airfoil
+solver iterations around the plan instead (fot_airfoil_run: the cell passes
+k_cells, k_bres_calc, k_rms and the plan's res_calc kernel).  Plan labels are those of cuda_fot_b200.tune.Candidate.label():
 `order[+partN]/exec[d][-plain]/block[@soa]`, e.g. `gps/hier/128`,
 `gps+part256/hierd/256`, `as-is/atomic-plain/256@soa`.  Sizes: res_calc/volna/getacc take --n as the grid edge
 (n x n), mini_aero/lulesh as the hex edge (n^3).
@@ -60,9 +62,24 @@ def main(argv=None) -> int:
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--plan", default="rcm/atomic/256")
     ap.add_argument("--launches", type=int, default=6)
+    ap.add_argument("--airfoil", action="store_true",
+                    help="res_calc only: run `--launches` Airfoil iterations (fot_airfoil_run) "
+                         "around the plan instead of bare loop iterations")
     a = ap.parse_args(argv)
     md = make_mesh(a.loop, a.n, a.seed)
     cand = parse_plan(a.plan)
+    if a.airfoil:
+        if a.loop != "res_calc":
+            raise SystemExit("--airfoil needs --loop res_calc")
+        from . import bench_configs as BC
+        ex = mg.airfoil_extras(md)
+        p, plan, af = BC.airfoil_setup(md, ex, cand)
+        rms = None
+        for _ in range(a.launches):
+            rms = af.run(plan, 1)
+        print(f"airfoil res_calc n={a.n} cells={md.n_points[0]} edges={md.n_cells} plan={cand.label()} "
+              f"iterations={a.launches} rms={rms}")
+        return 0
     cache = T.OrderedCache(md)
     p, plan = T.build(cache.get(cand.order, cand.partition, cand.layout), cand)
     for _ in range(a.launches):

@@ -318,6 +318,13 @@ int fot_airfoil_create(fot_problem *p, const fot_airfoil_desc *desc, fot_airfoil
 /* `iterations` solver iterations on `stream`; rms (host, may be NULL) receives
  * the last iteration's rms after the stream is synchronised. */
 int fot_airfoil_run(fot_airfoil *a, fot_plan *plan, uint32_t iterations, double *rms, void *stream);
+/* The whole time loop as one CUDA graph: `iterations` solver iterations
+ * captured from `stream` (the problem's numbering is brought up to date
+ * first); fot_graph_launch replays them, fot_airfoil_get_rms then reads the
+ * last iteration's rms (synchronising `stream`). */
+int fot_airfoil_graph_create(fot_airfoil *a, fot_plan *plan, uint32_t iterations, void *stream,
+                             fot_graph **out);
+int fot_airfoil_get_rms(fot_airfoil *a, double *rms, void *stream);
 int fot_airfoil_destroy(fot_airfoil *a);
 
 /* ---- batches: many meshes, one persistent launch -------------------------- */

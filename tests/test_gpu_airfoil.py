@@ -7,7 +7,8 @@ against its oracle (orc_airfoil_run):
 * with the atomic plan: within 1e-11 normwise of the oracle's serial order;
 * maps given in the original numbering follow a reordered problem, also
   when the problem is reordered after the Airfoil step was created;
-* bad input and a destroyed problem are refused with an error code.
+* bad input and a destroyed problem are refused with an error code;
+* the time loop captured as one CUDA graph replays to the same results.
 """
 import numpy as np
 import pytest
@@ -133,3 +134,35 @@ def test_destroyed_problem_is_refused():
     with pytest.raises(F().FotError) as e:
         af.run(plan, 1)
     assert e.value.code == -3  # FOT_ERR_STATE
+
+
+@pytest.mark.parametrize("exec_", ["hier", "atomic"])
+def test_graph_replays_the_time_loop(exec_):
+    """The time loop captured as one CUDA graph gives the run's results
+    (bit for bit with a coloured plan)."""
+    md = mg.res_calc(40, 32, 9)
+    ex = mg.airfoil_extras(md)
+    out = []
+    for use_graph in (False, True):
+        p = F().Problem.from_mesh(md)
+        plan = (p.plan(F().EXEC_HIER, 128) if exec_ == "hier"
+                else p.plan(F().EXEC_ATOMIC, 256, F().PLAN_NO_AGGREGATE))
+        af = airfoil(p, ex)
+        if use_graph:
+            g = af.graph(plan, 3)
+            g.launch()
+            g.launch()
+            rms = af.rms()
+        else:
+            af.run(plan, 3)
+            rms = af.run(plan, 3)
+        p.sync()
+        out.append((p.point_weights(2), rms))
+    if exec_ == "hier":
+        assert bitwise_equal(out[0][0], out[1][0])
+        assert out[0][1] == out[1][1]
+    else:
+        assert rel_err(out[1][0], out[0][0]) <= 1e-11
+    ref, ref_rms = O.airfoil(md, ex, 6)
+    assert rel_err(out[1][0], ref[2]) <= 1e-11
+    assert abs(out[1][1] - ref_rms) <= 1e-9 * ref_rms
