@@ -263,6 +263,7 @@ int fot_problem_destroy(fot_problem *p) {
   if (p) {
     for (fot_plan *plan : p->plans) plan->prob = nullptr;
     for (fot_airfoil *a : p->airfoils) fot_airfoil_detach(a);
+    for (fot_rowlist *l : p->rowlists) fot_rowlist_detach(l);
   }
   delete p;
   return FOT_OK;

@@ -96,6 +96,8 @@ struct fot_problem {
   std::vector<struct fot_plan *> plans;
   // live Airfoil steps on this problem (told when the problem is destroyed)
   std::vector<struct fot_airfoil *> airfoils;
+  // live row lists of this problem's datasets (told when it is destroyed)
+  std::vector<struct fot_rowlist *> rowlists;
 
   size_t point_bytes(uint32_t k) const {
     return (size_t)n_points[k] * info.point_dim[k] * info.point_type_size[k];
@@ -110,6 +112,8 @@ struct fot_problem {
 
 // An Airfoil step whose problem is being destroyed (fails from now on).
 void fot_airfoil_detach(struct fot_airfoil *a);
+// A row list whose problem is being destroyed (fails from now on).
+void fot_rowlist_detach(struct fot_rowlist *l);
 
 namespace fot {
 // Capture into a new fot_graph what enqueue(ctx, stream) launches (on a

@@ -215,6 +215,30 @@ class Batch:
             self._h = None
 
 
+class RowList:
+    """Distinct rows of point dataset k kept on the device (fot_rowlist):
+    gather packs them into a device buffer, scatter_add adds one in."""
+
+    def __init__(self, problem: "Problem", k: int, rows: np.ndarray):
+        self.problem = problem
+        r = np.ascontiguousarray(rows, dtype=np.uint32)
+        self.n = len(r)
+        self._h = C.c_void_p()
+        _check(_lib.fot_rowlist_create(problem._h, C.c_uint32(k), r.ctypes.data_as(u32p),
+                                       C.c_uint32(self.n), C.byref(self._h)))
+
+    def gather(self, dst_ptr: int, stream=None) -> None:
+        _check(_lib.fot_rowlist_gather(self._h, C.c_void_p(dst_ptr), _stream_ptr(stream)))
+
+    def scatter_add(self, src_ptr: int, stream=None) -> None:
+        _check(_lib.fot_rowlist_scatter_add(self._h, C.c_void_p(src_ptr), _stream_ptr(stream)))
+
+    def __del__(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.fot_rowlist_destroy(self._h)
+            self._h = None
+
+
 class AirfoilDesc(C.Structure):
     _fields_ = [("cell_to_node", u32p), ("n_bedges", C.c_uint32), ("bedge_to_node", u32p),
                 ("bedge_to_cell", u32p), ("bound", C.POINTER(C.c_int32)),

@@ -283,6 +283,24 @@ int fot_graph_create(fot_problem *p, fot_plan *plan, uint32_t iterations,
 int fot_graph_launch(fot_graph *g, void *stream);
 int fot_graph_destroy(fot_graph *g);
 
+/* ---- row lists: the device side of a partitioned (multi-GPU) run -------- */
+
+/* The reference runs one mesh on one GPU.  A mesh split by cells into parts
+ * (fot_partition) runs one part per GPU: each part's problem holds its cells
+ * and every point they touch; a point touched by several parts is owned by
+ * one, and the increments the others add to their copies travel to the owner
+ * after the loop (cuda_fot_b200/halo.py does the split and the exchange over
+ * torch.distributed).  A row list is a set of DISTINCT rows of point dataset
+ * k (current numbering, checked, kept on the device): gather packs them into
+ * `dst` (device, rows x dim elements, AOS, list order); scatter_add adds such
+ * a packed buffer into the dataset.  Lists become stale
+ * (FOT_ERR_STATE) when the problem is renumbered. */
+typedef struct fot_rowlist fot_rowlist;
+int fot_rowlist_create(fot_problem *p, uint32_t k, const uint32_t *rows, uint32_t n, fot_rowlist **out);
+int fot_rowlist_gather(const fot_rowlist *l, void *dst, void *stream);
+int fot_rowlist_scatter_add(const fot_rowlist *l, const void *src, void *stream);
+int fot_rowlist_destroy(fot_rowlist *l);
+
 /* ---- the Airfoil time step around res_calc ------------------------------ */
 
 /* The reference drives res_calc alone (res_calc.cu: Problem::loop*(num)).  An
