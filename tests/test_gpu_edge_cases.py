@@ -93,3 +93,22 @@ def test_refused_input():
     p = F().Problem.from_mesh(md)
     with pytest.raises(F().FotError):  # wrong dataset size
         p.set_point_data(0, np.zeros((3, 4)))
+
+
+@pytest.mark.parametrize("name", ["res_calc_58", "lulesh_27", "mini_aero_54"])
+@pytest.mark.parametrize("block", [1, 1024])
+def test_block_size_limits(name, block):
+    """The smallest (one cell per block) and largest block sizes run and
+    replay bit for bit; sizes outside [1, 1024] are refused."""
+    md = TINY[name]()
+    p = F().Problem.from_mesh(md)
+    plan = p.plan(F().EXEC_HIER, block, 0)
+    ex = plan.export()
+    plan.run(2)
+    p.sync()
+    rep, _ = O.replay_hier(md, ex, 2)
+    assert bitwise_equal(p.point_weights(0), rep[0])
+    for bad in (0, 1025):
+        with pytest.raises(F().FotError) as e:
+            p.plan(F().EXEC_HIER, bad, 0)
+        assert e.value.code == -1  # FOT_ERR_ARG
