@@ -413,6 +413,7 @@ int fot_airfoil_graph_create(fot_airfoil *a, fot_plan *plan, uint32_t iterations
   (*out)->prob = a->prob;
   (*out)->plan = plan;
   (*out)->ctl = plan->ctl.as<Ctl>();
+  (*out)->version = a->prob->version;
   return FOT_OK;
 }
 

@@ -656,13 +656,22 @@ int fot_graph_create(fot_problem *p, fot_plan *plan, uint32_t iterations, void *
   (*out)->prob = p;
   (*out)->plan = plan;
   (*out)->ctl = plan->ctl.as<Ctl>();
+  (*out)->version = p->version;
   return FOT_OK;
 }
 
 int fot_graph_launch(fot_graph *g, void *stream) {
   if (!g) return fail(FOT_ERR_ARG, "null graph");
+  // the graph replays the device addresses it was captured with: refuse it
+  // once its problem is gone or its buffers were replaced (renumbering,
+  // another plan's cell order, a layout change)
+  if (g->plan) {
+    if (!g->plan->prob) return fail(FOT_ERR_STATE, "the graph's problem was destroyed");
+    if (g->plan->prob->version != g->version)
+      return fail(FOT_ERR_STATE, "graph is stale: the problem was renumbered after the capture");
+  }
   FOT_CUDA(cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream)));
-  if (g->plan) note_run(g->prob, g->plan);
+  if (g->plan) note_run(g->plan->prob, g->plan);
   return FOT_OK;
 }
 

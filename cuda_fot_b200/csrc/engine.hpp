@@ -156,6 +156,8 @@ struct fot_graph {
   cudaGraphExec_t exec = nullptr;
   fot_problem *prob = nullptr;
   fot_plan *plan = nullptr;
+  // the problem's numbering at capture: the graph holds its buffers' addresses
+  uint64_t version = 0;
   fot::Ctl *ctl = nullptr;
   ~fot_graph() {
     if (exec) cudaGraphExecDestroy(exec);

@@ -112,3 +112,20 @@ def test_block_size_limits(name, block):
         with pytest.raises(F().FotError) as e:
             p.plan(F().EXEC_HIER, bad, 0)
         assert e.value.code == -1  # FOT_ERR_ARG
+
+
+@pytest.mark.parametrize("exec_", [0, 1])
+def test_stale_graph_is_refused(exec_):
+    """A captured graph replays the buffers it was captured with: after the
+    problem is renumbered its launch is refused, not replayed."""
+    md = mg.res_calc(10, 8, 1)
+    p = F().Problem.from_mesh(md)
+    plan = p.plan(exec_, 256 if exec_ == 0 else 64, 0)
+    g = plan.graph(2)
+    g.launch()
+    p.sync()
+    p.reorder(F().ORDER_RCM)
+    with pytest.raises(F().FotError) as e:
+        g.launch()
+    assert e.value.code == -3  # FOT_ERR_STATE
+    del g
