@@ -268,7 +268,7 @@ def main(argv=None):
     stream = torch.cuda.current_stream()
 
     # plan choice: the cost model's pick when a trained model is present, else
-    # the measured sweep; the sweep also judges the model's pick (regret)
+    # the measured sweep; the sweep also measures the model's pick (regret)
     from cuda_fot_b200.profile_case import parse_plan
     choice_src = "sweep"
     choice_note = None
@@ -294,7 +294,7 @@ def main(argv=None):
     sweep_res = []
     if choice_src != "forced":
         # the exhaustive measured sweep over the same candidates the model
-        # picks from: the fallback, and the judge of the model's pick
+        # picks from: the fallback, and the yardstick of the model's pick
         cands = T.default_candidates(md.loop)
         if chosen is not None and chosen.label() not in [c.label() for c in cands]:
             cands.append(chosen)

@@ -9,7 +9,7 @@ cuda_fot_b200.tune.Candidate),
 relative to the mean over the candidates timed on the same mesh, from
 features of the mesh AFTER the candidate's ordering and of the plan.  The
 autotuner's exhaustive measured sweep generates the training data and stays
-as the fallback and the judge: the model's pick is compared with the sweep's
+as the fallback and the yardstick: the model's pick is compared with the sweep's
 best (regret) and with a fixed default plan (what the model gains).
 
 Features (FEATURES below): mesh size and bytes, the loop kind, the histogram

@@ -15,7 +15,7 @@ A candidate is (ordering, partition size, executor, block size, layout):
 
 ``measure(md, cand)`` builds the candidate on a fresh problem and times
 ``iters`` iterations with CUDA events on the launching stream after warm-up.
-The exhaustive sweep over a candidate list is the fallback and the judge of
+The exhaustive sweep over a candidate list is the fallback and the yardstick of
 the learned cost model (cuda_fot_b200/costmodel.py), and it produces that
 model's training data.
 """
