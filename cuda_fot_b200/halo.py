@@ -24,6 +24,7 @@ flows the other way.
 """
 from __future__ import annotations
 
+from contextlib import nullcontext
 from dataclasses import dataclass, field
 from typing import Callable, Dict, List, Optional
 
@@ -140,7 +141,8 @@ def assemble(md: mg.MeshData, locals_: List[LocalMesh], results: List[np.ndarray
 class PartitionedLoop:
     """A rank's part on its GPU: the engine problem of lm.md, its plan, and
     device row lists of the halo rows it sends and the owned rows it
-    receives.  run(k) = k loop iterations, then the halo exchange."""
+    receives.  run(k) = k loop iterations, then the halo exchange; `stream`
+    is a torch.cuda.Stream or None (torch's current stream)."""
 
     def __init__(self, lm: LocalMesh, exec: int, block_size: int = 256, flags: int = 0,
                  order: Optional[int] = None, group=None):
@@ -169,8 +171,12 @@ class PartitionedLoop:
         def scatter_add(s, t):
             self.recv[s].scatter_add(t.data_ptr(), stream)
 
-        exchange(self.lm, gather, scatter_add,
-                 lambda n: torch.empty(n, dtype=dt, device="cuda"), self.group)
+        # the collective is ordered after torch's current stream: issue it
+        # under the stream the loop and the row kernels run on
+        ctx = torch.cuda.stream(stream) if isinstance(stream, torch.cuda.Stream) else nullcontext()
+        with ctx:
+            exchange(self.lm, gather, scatter_add,
+                     lambda n: torch.empty(n, dtype=dt, device="cuda"), self.group)
 
     def result(self) -> np.ndarray:
         """Point dataset 0 in the local numbering (host)."""
