@@ -31,7 +31,10 @@
  *     (the order of res_calc.hpp:319-358);
  *   - orc_check_plan: exact integer checks of a plan;
  *   - orc_point_graph / orc_reorder_inverse: the point-to-point CSR graph of a
- *     mapping (reorder.hpp:33-132, 177-202), pinned by the reference's Catch KAT.
+ *     mapping (reorder.hpp:33-132, 177-202), pinned by the reference's Catch KAT;
+ *   - orc_airfoil_run: the Airfoil solver iteration the engine runs around
+ *     res_calc (its other loops are not in the reference: pinned instead to
+ *     an independent Python statement in the tests).
  */
 #ifndef FOT_ORACLE_H
 #define FOT_ORACLE_H
