@@ -282,7 +282,9 @@ int fot_graph_create(fot_problem *p, fot_plan *plan, uint32_t iterations,
                      void *stream, fot_graph **out);
 /* A graph replays the device addresses it was captured with: once its
  * problem is renumbered (fot_reorder, another plan build, fot_set_layout,
- * ...) or destroyed, fot_graph_launch refuses it with FOT_ERR_STATE. */
+ * ...) or destroyed, fot_graph_launch refuses it with FOT_ERR_STATE.  A
+ * graph must be destroyed before the plan (and the Airfoil step) it was
+ * captured from. */
 int fot_graph_launch(fot_graph *g, void *stream);
 int fot_graph_destroy(fot_graph *g);
 
